@@ -1,0 +1,214 @@
+/*
+ * sppgpu.h — C ABI of the B200 filterbank dedispersion library (libsppgpu.so).
+ *
+ * Plain C: pointers, sizes and status codes only.  Every entry point returns
+ * an int status (SPP_OK == 0, negative on error) and, on error, leaves a
+ * message for spp_last_error_string() in thread-local storage.
+ *
+ * Conventions
+ *   - Unless stated otherwise every data pointer is a DEVICE pointer owned by
+ *     the caller (e.g. a torch tensor's data_ptr()).  The "_host" entry points
+ *     take host buffers and do their own copies.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Device work is stream-ordered; nothing synchronises unless the
+ *     function says so.
+ *   - Hot calls allocate nothing: scratch space ("workspace") is sized by the
+ *     matching *_workspace_bytes() call and passed in by the caller.  Plans
+ *     (spp_dmt_plan_*) allocate their device tables once at creation.
+ *   - Filterbank input is the raw sigproc stream: time-major, `nchans`
+ *     samples per spectrum, `nbits` in {1, 2, 4, 8} (packed, uint8 container)
+ *     or 32 (float32).  `bitorder` is SPP_BITORDER_BIG or _LITTLE for packed
+ *     data (sample k of a byte holds channel k of that byte's group).
+ *
+ * Each entry point names the reference interface it replaces
+ * (FRBs/sigpyproc3, paths relative to src/sigpyproc/).
+ */
+#ifndef SPPGPU_H
+#define SPPGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define SPP_OK 0
+#define SPP_ERR_ARG (-1)         /* bad argument (null pointer, bad enum)       */
+#define SPP_ERR_SIZE (-2)        /* buffer too small / shape inconsistent       */
+#define SPP_ERR_ALIGN (-3)       /* pointer alignment requirement not met       */
+#define SPP_ERR_CUDA (-4)        /* a CUDA runtime call failed                  */
+#define SPP_ERR_TIMEOUT (-5)     /* a device-side bounded wait expired          */
+#define SPP_ERR_UNSUPPORTED (-6) /* valid request outside what is implemented   */
+#define SPP_ERR_DELAY (-7)       /* delay table out of the representable range  */
+#define SPP_ERR_DEVICE (-8)      /* device status word reported an error        */
+
+#define SPP_BITORDER_BIG 0
+#define SPP_BITORDER_LITTLE 1
+
+/* output element kinds */
+#define SPP_OUT_F32 0 /* float32 samples                                       */
+#define SPP_OUT_I32 1 /* int32 sums (integer input only; exact)                */
+
+/* delay application modes for the DM-time transform */
+#define SPP_MODE_DEDISPERSE 0 /* out[t] = sum_c x[t + d_c][c]   (kernels.dedisperse) */
+#define SPP_MODE_ROLL 1       /* out[t] = sum_c x[(t - d_c) mod n][c] (kernels.dmt_block) */
+
+/* float accumulation for float32 input */
+#define SPP_ACC_KAHAN32 0 /* compensated fp32 (Kahan 1965)                       */
+#define SPP_ACC_F64 1     /* fp64 accumulator, as the reference kernels          */
+
+const char* spp_last_error_string(void);
+int spp_version(void);
+
+/* Device status word helpers: kernels record bounded-wait timeouts and
+ * defensive range checks in a 16-byte device status block (4 x uint32) that
+ * lives at the start of every workspace.  spp_status_read copies it to
+ * `host_out[4]` (synchronising `stream`) and returns SPP_OK, or SPP_ERR_DEVICE
+ * if word 0 is non-zero. */
+int spp_status_read(const void* workspace, uint32_t* host_out, void* stream);
+int spp_status_clear(void* workspace, void* stream);
+
+/* ---- R4: unpack -------------------------------------------------------------
+ * Replaces kernels.unpack{1,2,4}_8_{big,little} (core/kernels.py:20-69) and
+ * io/bits.py unpack (:19-70): `nbytes` packed bytes -> nbytes*8/nbits uint8
+ * samples, sample k of byte i written to out[i*8/nbits + k]. */
+int spp_unpack(const uint8_t* in, int64_t nbytes, int nbits, int bitorder,
+               uint8_t* out, void* stream);
+
+/* ---- R2: single-DM dedispersion ---------------------------------------------
+ * Replaces kernels.dedisperse / dedisperse_par (core/kernels.py:340-362, :542):
+ *   out[out_start + t] = sum_c x[t + delays[c]][c],  t < nsamps - max|delays|
+ * with negative row indices wrapping within the block (numba semantics).
+ * Integer input is summed exactly; float32 input with `acc` (SPP_ACC_F64
+ * matches the reference's float64 accumulator).  `delays` is a device int32
+ * array of nchans entries; delay_min/delay_max are its min and max (the host
+ * knows them; the kernel range-checks every entry against them).
+ * `out_len` is the full length of `out`; the call fails with SPP_ERR_SIZE if
+ * out_start + nsamps - max|d| > out_len (the reference has no such check). */
+int64_t spp_dedisperse_workspace_bytes(int nbits, int64_t nchans, int64_t nsamps,
+                                       int32_t delay_min, int32_t delay_max);
+int spp_dedisperse(const void* in, int nbits, int bitorder, int64_t nchans,
+                   int64_t nsamps, const int32_t* delays, int32_t delay_min,
+                   int32_t delay_max, float* out, int64_t out_len,
+                   int64_t out_start, int acc, void* workspace,
+                   int64_t workspace_bytes, void* stream);
+
+/* ---- R3: DM-trial batch (DM-time transform) -----------------------------------
+ * Replaces FilterbankBlock.dmt_transform (block.py:309-343) / kernels.dmt_block
+ * (core/kernels.py:1155-1168).  A plan owns the ndm x nchans delay table on the
+ * device and the tile geometry; execute runs
+ *   SPP_MODE_DEDISPERSE: out[i][t] = sum_c x[t + D[i][c]][c], t < nsamps - max|D|
+ *   SPP_MODE_ROLL:       out[i][t] = sum_c x[(t - D[i][c]) mod nsamps][c], t < nsamps
+ * writing rows of `out` with row stride `out_stride` elements starting at
+ * column `out_start`.  delays_host is a host int32 array (ndm x nchans,
+ * row-major), read once at plan creation. */
+typedef struct spp_dmt_plan spp_dmt_plan;
+int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder,
+                        int64_t nchans, int64_t nsamps_max, int64_t ndm,
+                        const int32_t* delays_host, int mode, int out_kind,
+                        int acc);
+int spp_dmt_plan_destroy(spp_dmt_plan* plan);
+/* valid output samples per row for an input of `nsamps` samples */
+int64_t spp_dmt_plan_nvalid(const spp_dmt_plan* plan, int64_t nsamps);
+int64_t spp_dmt_plan_workspace_bytes(const spp_dmt_plan* plan, int64_t nsamps);
+/* describe the chosen tiles: fills cfg[8] = {nbits, R, DW, TW, SLAB, STAGES,
+ * T (samples per tile), smem bytes} */
+int spp_dmt_plan_describe(const spp_dmt_plan* plan, int32_t* cfg);
+/* override the tile shape (autotuner); variant index in [0, n) */
+int spp_dmt_plan_num_variants(const spp_dmt_plan* plan);
+int spp_dmt_plan_set_variant(spp_dmt_plan* plan, int variant);
+int spp_dmt_execute(const spp_dmt_plan* plan, const void* in, int64_t nsamps,
+                    void* out, int64_t out_stride, int64_t out_start,
+                    void* workspace, int64_t workspace_bytes, void* stream);
+/* Same transform end to end from HOST memory: `in_host` (pinned or pageable)
+ * and `out_host` (ndm x out_stride elements).  Time is cut into blocks of
+ * `block_nsamps` output samples; H2D, compute and D2H of successive blocks
+ * overlap on two internal streams.  Synchronous: returns when out_host is
+ * complete. */
+int spp_dmt_execute_host(const spp_dmt_plan* plan, const void* in_host,
+                         int64_t nsamps, void* out_host, int64_t out_stride,
+                         int64_t block_nsamps, void* workspace,
+                         int64_t workspace_bytes);
+int64_t spp_dmt_host_workspace_bytes(const spp_dmt_plan* plan,
+                                     int64_t block_nsamps);
+
+/* ---- R10 / N2: channel statistics and zero-DM --------------------------------
+ * spp_bandpass: kernels.extract_bpass (core/kernels.py:281-292): bpass[c] +=
+ * sum_t x[t][c], accumulated sequentially in float32 per channel exactly as the
+ * reference loop (bit-identical).  spp_collapse: kernels.extract_tim
+ * (core/kernels.py:255-278): tim[out_start + t] += sum_c x[t][c] (float64
+ * accumulator, stored float32).  spp_zero_dm: kernels.remove_zerodm
+ * (core/kernels.py:465-505) for float32 input:
+ *   y[t][c] = f32((f64(x) - zdm[t] * f64(bpass[c]/sum(bpass))) + f64(bpass[c]))
+ * with zdm[t] = sum_c f64(x[t][c]); `chanwts` is bpass/sum(bpass) computed by
+ * the caller in float32 (as the reference). */
+int spp_bandpass(const void* in, int nbits, int bitorder, int64_t nchans,
+                 int64_t nsamps, float* bpass, void* stream);
+int spp_collapse(const void* in, int nbits, int bitorder, int64_t nchans,
+                 int64_t nsamps, float* tim, int64_t out_start, void* stream);
+int spp_zero_dm(const float* in, float* out, int64_t nchans, int64_t nsamps,
+                const float* bpass, const float* chanwts, void* stream);
+
+/* ---- R8: downsample ----------------------------------------------------------
+ * kernels.downsample_1d_mean (core/kernels.py:176-204): out[i] =
+ * f32(sum_{k<factor} f64(in[i*factor+k]) / factor) for i < n / factor, for
+ * `nrows` independent rows of `n` samples (row strides in elements). */
+int spp_downsample_mean(const float* in, int64_t nrows, int64_t n,
+                        int64_t in_stride, int factor, float* out,
+                        int64_t out_stride, void* stream);
+/* kernels.downsample_2d_mean_flat (core/kernels.py:207-252) */
+int spp_downsample_2d_mean(const float* in, int64_t dim1, int64_t dim2,
+                           int factor1, int factor2, float* out, void* stream);
+
+/* ---- R9: boxcar matched filter -> S/N peaks ------------------------------------
+ * For each of `nrows` rows (row stride `in_stride` elements, `n` valid samples,
+ * element kind in_kind = SPP_OUT_F32 or SPP_OUT_I32), for each downsample
+ * factor f in factors[0..nfactors) and boxcar width w in widths[0..nwidths)
+ * (HOST arrays; nfactors <= 8, nwidths <= 32, 1 <= w <= 4096):
+ *   y = downsample_1d_mean(row, f)   (length n_f = n / f)
+ *   mean, std = of y (float64, population std)
+ *   snr = max_{t <= n_f - w} (sum_{k<w} y[t+k] - w*mean) / (std * sqrt(w))
+ * written to snr[row][fi][wi] (float32) and, if `peak_index` is not NULL, the
+ * argmax t to peak_index[row][fi][wi] (int32).  Semantics follow
+ * TimeSeries.downsample + apply_boxcar (timeseries.py:107-132, :296-325) on a
+ * z-scored series (stats.estimate_zscore, core/stats.py:418-477, loc=mean,
+ * scale=std). */
+int64_t spp_boxcar_snr_workspace_bytes(int64_t nrows, int64_t n, int nfactors,
+                                       int nwidths);
+int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n,
+                   int64_t in_stride, const int32_t* factors, int nfactors,
+                   const int32_t* widths, int nwidths, float* snr,
+                   int32_t* peak_index, void* workspace,
+                   int64_t workspace_bytes, void* stream);
+
+/* ---- R7: subband dedispersion ----------------------------------------------------
+ * Stage 1 replaces kernels.subband (core/kernels.py:379-401) with a zeroed
+ * output: out[t][s] = sum_{c: chan_to_sub[c]==s} x[t + delays[c]][c] for
+ * t < nsamps - maxdelay, (nsamps - maxdelay) x nsub float32, row-major.
+ * `delays` and `chan_to_sub` are device int32 arrays of nchans entries. */
+int spp_subband(const void* in, int nbits, int bitorder, int64_t nchans,
+                int64_t nsamps, const int32_t* delays, int32_t maxdelay,
+                const int32_t* chan_to_sub, int64_t nsub, float* out,
+                void* stream);
+
+/* ---- Synthetic inputs (benchmark / test data; no reference counterpart) -------
+ * Counter-based generators: element i depends only on (seed, start + i)
+ * through the SplitMix64 finaliser, so slices can be regenerated on the host.
+ * spp_synth_gauss_u8 maps the upper 32 hash bits through 255 uint32 CDF
+ * thresholds (host array); spp_synth_pulse_packed adds +1 (saturating) to the
+ * packed field of channel c for rows start_rows[c] .. + width - 1. */
+int spp_synth_uniform_bytes(uint8_t* out, int64_t start, int64_t n, uint64_t seed,
+                            void* stream);
+int spp_synth_gauss_u8(uint8_t* out, int64_t start, int64_t n, uint64_t seed,
+                       const uint32_t* thresholds_host, void* stream);
+int spp_synth_gauss_f32(float* out, int64_t start, int64_t n, uint64_t seed, float mean,
+                        float stdv, void* stream);
+int spp_synth_pulse_packed(uint8_t* raw, int64_t nchans, int64_t nsamps, int nbits,
+                           int bitorder, const int64_t* start_rows, int width, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPPGPU_H */

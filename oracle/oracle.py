@@ -1,0 +1,245 @@
+"""ctypes bindings for the C oracle plus numpy restatements -- TEST INFRASTRUCTURE.
+
+Every function restates a reference routine (FRBs/sigpyproc3,
+``src/sigpyproc/...``) on the CPU; the file:line it follows is given in each
+docstring.  These are the checkers for the CUDA library, never the product.
+The restatements are pinned against the reference's own outputs by the
+fixtures in ``tests/golden/``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+
+_i64 = ctypes.c_int64
+_i32 = ctypes.c_int32
+_p = ctypes.c_void_p
+
+
+def build(force: bool = False) -> Path:
+    src = HERE / "spp_oracle.c"
+    if force or not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-s", "-B" if force else "-s", "-C", str(HERE), "liboracle.so"],
+                       check=True)
+    return LIB
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(str(LIB))
+        sig = {
+            "orc_set_threads": ([ctypes.c_int], None),
+            "orc_max_threads": ([], ctypes.c_int),
+            "orc_unpack": ([_p, _i64, ctypes.c_int, ctypes.c_int, _p], None),
+            "orc_dedisperse_u8": ([_p, _p, _p, _i64, _i64, _i64], _i64),
+            "orc_dedisperse_f32": ([_p, _p, _p, _i64, _i64, _i64], _i64),
+            "orc_dmt_u8_i32": ([_p, _p, _i64, _i64, _i64, _i64, _p, _i64], None),
+            "orc_dmt_f32": ([_p, _p, _i64, _i64, _i64, _i64, _p, _p, _i64], None),
+            "orc_dmt_roll_f32": ([_p, _p, _i64, _i64, _i64, _p], None),
+            "orc_dmt_packed_i32": ([_p, ctypes.c_int, ctypes.c_int, _p, _i64, _i64, _i64, _i64,
+                                    _p, _i64], None),
+            "orc_bandpass_f32": ([_p, _i64, _i64, _p], None),
+            "orc_bandpass_u8": ([_p, _i64, _i64, _p], None),
+            "orc_collapse_f32": ([_p, _i64, _i64, _p, _i64], None),
+            "orc_zero_dm_f32": ([_p, _p, _i64, _i64, _p, _p], None),
+            "orc_downsample_mean": ([_p, _i64, ctypes.c_int, _p], None),
+            "orc_boxcar_snr_row": ([_p, _i64, _p, ctypes.c_int, _p, ctypes.c_int, _p, _p], None),
+            "orc_subband_u8": ([_p, _p, _p, _p, _i64, _i64, _i64, _i64], None),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.flags.c_contiguous
+    return a.ctypes.data
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+# ---------------------------------------------------------------------------
+# R6: delays.  params.compute_dmdelays (params.py:26-62) with
+# Header.chan_freqs (header.py:228-237): float32 NumPy arithmetic, the same
+# expression order, round-half-even, int32.
+# ---------------------------------------------------------------------------
+DM_CONSTANT_LK = 4.148808e3
+
+
+def chan_freqs(nchans: int, fch1: float, foff: float) -> np.ndarray:
+    return np.arange(nchans, dtype=np.float32) * foff + fch1
+
+
+def dmdelays(freqs, dm, tsamp: float, ref_freq: float, *, in_samples: bool = True):
+    freqs = np.atleast_1d(freqs).astype(np.float32)
+    dm = np.atleast_1d(dm)[:, np.newaxis].astype(np.float32)
+    delays = dm * DM_CONSTANT_LK * ((freqs**-2) - (ref_freq**-2))
+    if in_samples:
+        delays = (delays / tsamp).round().astype(np.int32)
+    return delays.squeeze()
+
+
+# ---------------------------------------------------------------------------
+# kernels wrappers
+# ---------------------------------------------------------------------------
+def unpack(packed: np.ndarray, nbits: int, bitorder: str = "big") -> np.ndarray:
+    """kernels.unpack{1,2,4}_8_{big,little} (core/kernels.py:20-69)."""
+    packed = np.ascontiguousarray(packed, dtype=np.uint8)
+    out = np.empty(packed.size * 8 // nbits, dtype=np.uint8)
+    lib().orc_unpack(_ptr(packed), packed.size, nbits, int(bitorder == "big"), _ptr(out))
+    return out
+
+
+def dedisperse(data: np.ndarray, delays: np.ndarray, nchans: int, nsamps: int,
+               out: np.ndarray | None = None, out_start: int = 0) -> np.ndarray:
+    """kernels.dedisperse (core/kernels.py:340-362) on a flat (nsamps*nchans) block."""
+    data = np.ascontiguousarray(data)
+    delays = np.ascontiguousarray(delays, dtype=np.int32)
+    nvalid = nsamps - int(np.max(np.abs(delays)))
+    if out is None:
+        out = np.zeros(max(nvalid, 0) + out_start, dtype=np.float32)
+    if data.dtype == np.uint8:
+        lib().orc_dedisperse_u8(_ptr(data), _ptr(out), _ptr(delays), nchans, nsamps, out_start)
+    elif data.dtype == np.float32:
+        lib().orc_dedisperse_f32(_ptr(data), _ptr(out), _ptr(delays), nchans, nsamps, out_start)
+    else:
+        raise TypeError(data.dtype)
+    return out
+
+
+def dmt(data: np.ndarray, delays: np.ndarray, nchans: int, nsamps: int,
+        nvalid: int | None = None, want64: bool = False):
+    """Row-wise DM batch: out[i] = kernels.dedisperse(data, delays[i])[:nvalid]."""
+    data = np.ascontiguousarray(data)
+    delays = np.ascontiguousarray(np.atleast_2d(delays), dtype=np.int32)
+    ndm = delays.shape[0]
+    if nvalid is None:
+        nvalid = nsamps - int(np.max(np.abs(delays)))
+    if data.dtype == np.uint8:
+        out = np.zeros((ndm, nvalid), dtype=np.int32)
+        lib().orc_dmt_u8_i32(_ptr(data), _ptr(delays), ndm, nchans, nsamps, nvalid, _ptr(out), nvalid)
+        return out
+    out = np.zeros((ndm, nvalid), dtype=np.float32)
+    out64 = np.zeros((ndm, nvalid), dtype=np.float64) if want64 else None
+    lib().orc_dmt_f32(_ptr(data), _ptr(delays), ndm, nchans, nsamps, nvalid, _ptr(out),
+                      _ptr(out64) if want64 else None, nvalid)
+    return (out, out64) if want64 else out
+
+
+def dmt_packed(packed: np.ndarray, nbits: int, bitorder: str, delays: np.ndarray, nchans: int,
+               nsamps: int, nvalid: int) -> np.ndarray:
+    packed = np.ascontiguousarray(packed, dtype=np.uint8)
+    delays = np.ascontiguousarray(np.atleast_2d(delays), dtype=np.int32)
+    ndm = delays.shape[0]
+    out = np.zeros((ndm, nvalid), dtype=np.int32)
+    lib().orc_dmt_packed_i32(_ptr(packed), nbits, int(bitorder == "big"), _ptr(delays), ndm,
+                             nchans, nsamps, nvalid, _ptr(out), nvalid)
+    return out
+
+
+def dmt_roll(data_tm: np.ndarray, delays: np.ndarray, nchans: int, nsamps: int) -> np.ndarray:
+    """kernels.dmt_block (core/kernels.py:1155-1168) on time-major float32 data."""
+    data_tm = np.ascontiguousarray(data_tm, dtype=np.float32)
+    delays = np.ascontiguousarray(np.atleast_2d(delays), dtype=np.int32)
+    out = np.zeros((delays.shape[0], nsamps), dtype=np.float32)
+    lib().orc_dmt_roll_f32(_ptr(data_tm), _ptr(delays), delays.shape[0], nchans, nsamps, _ptr(out))
+    return out
+
+
+def bandpass(data: np.ndarray, nchans: int, nsamps: int, bpass: np.ndarray | None = None):
+    """kernels.extract_bpass (core/kernels.py:281-292), sequential float32."""
+    bpass = np.zeros(nchans, np.float32) if bpass is None else bpass
+    data = np.ascontiguousarray(data)
+    fn = lib().orc_bandpass_u8 if data.dtype == np.uint8 else lib().orc_bandpass_f32
+    fn(_ptr(data), nchans, nsamps, _ptr(bpass))
+    return bpass
+
+
+def collapse(data: np.ndarray, nchans: int, nsamps: int, tim: np.ndarray, out_start: int = 0):
+    """kernels.extract_tim (core/kernels.py:255-278) for float32 data."""
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    lib().orc_collapse_f32(_ptr(data), nchans, nsamps, _ptr(tim), out_start)
+    return tim
+
+
+def zero_dm(data: np.ndarray, nchans: int, nsamps: int, bpass: np.ndarray) -> np.ndarray:
+    """kernels.remove_zerodm (core/kernels.py:465-505), float32 data."""
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    bpass = np.ascontiguousarray(bpass, dtype=np.float32)
+    chanwts = bpass / bpass.sum()
+    out = np.empty_like(data)
+    lib().orc_zero_dm_f32(_ptr(data), _ptr(out), nchans, nsamps, _ptr(bpass), _ptr(chanwts))
+    return out
+
+
+def downsample_mean(x: np.ndarray, factor: int) -> np.ndarray:
+    """kernels.downsample_1d_mean (core/kernels.py:176-204)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty(x.size // factor, dtype=np.float32)
+    lib().orc_downsample_mean(_ptr(x), x.size, factor, _ptr(out))
+    return out
+
+
+def boxcar_snr(rows: np.ndarray, factors, widths):
+    """Boxcar S/N peaks per row (float64) and argmax indices."""
+    rows = np.atleast_2d(rows)
+    factors = np.ascontiguousarray(factors, dtype=np.int32)
+    widths = np.ascontiguousarray(widths, dtype=np.int32)
+    snr = np.zeros((rows.shape[0], factors.size, widths.size), dtype=np.float64)
+    idx = np.zeros(snr.shape, dtype=np.int32)
+    for r in range(rows.shape[0]):
+        row = np.ascontiguousarray(rows[r], dtype=np.float32)
+        lib().orc_boxcar_snr_row(_ptr(row), row.size, _ptr(factors), factors.size, _ptr(widths),
+                                 widths.size, snr[r].ctypes.data, idx[r].ctypes.data)
+    return snr, idx
+
+
+def subband(data: np.ndarray, delays: np.ndarray, chan_to_sub: np.ndarray, maxdelay: int,
+            nchans: int, nsub: int, nsamps: int) -> np.ndarray:
+    """kernels.subband (core/kernels.py:379-401) with a zeroed output."""
+    data = np.ascontiguousarray(data, dtype=np.uint8)
+    delays = np.ascontiguousarray(delays, dtype=np.int32)
+    chan_to_sub = np.ascontiguousarray(chan_to_sub, dtype=np.int32)
+    out = np.zeros((nsamps - maxdelay) * nsub, dtype=np.float32)
+    lib().orc_subband_u8(_ptr(data), _ptr(out), _ptr(delays), _ptr(chan_to_sub), maxdelay,
+                         nchans, nsub, nsamps)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# readers.FilReader.read_plan schedule (readers.py:182-216)
+# ---------------------------------------------------------------------------
+def read_plan_blocks(nsamples: int, gulp: int = 16384, start: int = 0, nsamps: int | None = None,
+                     skipback: int = 0) -> list[tuple[int, int, int]]:
+    """(ii, samples in block, skip) for each block, or ValueError as the reference."""
+    if nsamps is None:
+        nsamps = nsamples - start
+    gulp = min(nsamps, gulp)
+    skipback = abs(skipback)
+    if skipback >= gulp:
+        raise ValueError(f"readsamps ({gulp}) must be > skipback ({skipback})")
+    nreads, lastread = divmod(nsamps, (gulp - skipback))
+    if lastread < skipback:
+        nreads -= 1
+        lastread = nsamps - (nreads * (gulp - skipback))
+    blocks = [(ii, gulp, -skipback) for ii in range(nreads)]
+    if lastread != 0:
+        blocks.append((nreads, lastread, 0))
+    return blocks

@@ -1,0 +1,269 @@
+/*
+ * CPU oracle for the sigpyproc dedispersion path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Plain-C restatements of the reference algorithms (FRBs/sigpyproc3, paths
+ * relative to src/sigpyproc/), used by tests/ to check the CUDA library, by
+ * __graft_entry__.smoke() as its checker and by bench.py's CPU-baseline leg.
+ * The product never links or calls this file.  Parity of these
+ * restatements with the reference's own code is pinned by the golden vectors
+ * in tests/golden/ (generated by running the reference numba kernels).
+ *
+ * Float sums are accumulated in double in channel order (no fast-math), as
+ * the reference kernels declare (np.float64 accumulators); the reference's
+ * fastmath may reassociate, which is below float32 resolution.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+static int g_threads = 1;
+
+void orc_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+int orc_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* kernels.unpack{1,2,4}_8_{big,little} (core/kernels.py:20-69): sample k of
+ * byte i -> out[i*per + k]; big order puts sample 0 in the high bits. */
+void orc_unpack(const uint8_t* in, int64_t nbytes, int nbits, int big, uint8_t* out) {
+  const int per = 8 / nbits;
+  const unsigned mask = (1u << nbits) - 1u;
+  for (int64_t i = 0; i < nbytes; ++i) {
+    const unsigned b = in[i];
+    for (int k = 0; k < per; ++k) {
+      const int sh = big ? (8 - (k + 1) * nbits) : (k * nbits);
+      out[i * per + k] = (uint8_t)((b >> sh) & mask);
+    }
+  }
+}
+
+/* numba array indexing wraps negative indices once (index + size). */
+static inline int64_t wrap_neg(int64_t i, int64_t n) { return i < 0 ? i + n : i; }
+
+static int32_t max_abs(const int32_t* d, int64_t n) {
+  int32_t m = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const int32_t a = d[i] < 0 ? -d[i] : d[i];
+    if (a > m) m = a;
+  }
+  return m;
+}
+
+/* kernels.dedisperse (core/kernels.py:340-362), uint8 input:
+ *   out[out_start + t] = sum_c in[(t + d_c) * nchans + c], t < nsamps - max|d|,
+ * float64 accumulator stored as float32.  Returns the number of outputs. */
+int64_t orc_dedisperse_u8(const uint8_t* in, float* out, const int32_t* delays, int64_t nchans,
+                          int64_t nsamps, int64_t out_start) {
+  const int64_t nvalid = nsamps - max_abs(delays, nchans);
+  for (int64_t t = 0; t < nvalid; ++t) {
+    double s = 0.0;
+    for (int64_t c = 0; c < nchans; ++c) s += in[wrap_neg(t + delays[c], nsamps) * nchans + c];
+    out[out_start + t] = (float)s;
+  }
+  return nvalid > 0 ? nvalid : 0;
+}
+
+/* Same for float32 input. */
+int64_t orc_dedisperse_f32(const float* in, float* out, const int32_t* delays, int64_t nchans,
+                           int64_t nsamps, int64_t out_start) {
+  const int64_t nvalid = nsamps - max_abs(delays, nchans);
+  for (int64_t t = 0; t < nvalid; ++t) {
+    double s = 0.0;
+    for (int64_t c = 0; c < nchans; ++c)
+      s += (double)in[wrap_neg(t + delays[c], nsamps) * nchans + c];
+    out[out_start + t] = (float)s;
+  }
+  return nvalid > 0 ? nvalid : 0;
+}
+
+/* DM-trial batch, row-wise R2 contract: out[i][t] = dedisperse(x, D[i])[t]
+ * for t < nvalid (= nsamps - max over all |D|), uint8 input, exact int32
+ * sums.  Parallel over DM rows. */
+void orc_dmt_u8_i32(const uint8_t* in, const int32_t* delays, int64_t ndm, int64_t nchans,
+                    int64_t nsamps, int64_t nvalid, int32_t* out, int64_t out_stride) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads)
+  for (int64_t i = 0; i < ndm; ++i) {
+    const int32_t* d = delays + i * nchans;
+    int32_t* o = out + i * out_stride;
+    for (int64_t t = 0; t < nvalid; ++t) o[t] = 0;
+    for (int64_t c = 0; c < nchans; ++c) {
+      const uint8_t* col = in + c;
+      const int64_t dc = d[c];
+      for (int64_t t = 0; t < nvalid; ++t) o[t] += col[wrap_neg(t + dc, nsamps) * nchans];
+    }
+  }
+}
+
+/* Float32 input: float64 sum per output in channel order, stored float32
+ * (and optionally float64 in out64). */
+void orc_dmt_f32(const float* in, const int32_t* delays, int64_t ndm, int64_t nchans,
+                 int64_t nsamps, int64_t nvalid, float* out, double* out64, int64_t out_stride) {
+#pragma omp parallel num_threads(g_threads)
+  {
+    double* acc = (double*)malloc(sizeof(double) * (nvalid > 0 ? nvalid : 1));
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t i = 0; i < ndm; ++i) {
+      const int32_t* d = delays + i * nchans;
+      for (int64_t t = 0; t < nvalid; ++t) acc[t] = 0.0;
+      for (int64_t c = 0; c < nchans; ++c) {
+        const float* col = in + c;
+        const int64_t dc = d[c];
+        for (int64_t t = 0; t < nvalid; ++t) acc[t] += (double)col[wrap_neg(t + dc, nsamps) * nchans];
+      }
+      for (int64_t t = 0; t < nvalid; ++t) {
+        if (out) out[i * out_stride + t] = (float)acc[t];
+        if (out64) out64[i * out_stride + t] = acc[t];
+      }
+    }
+    free(acc);
+  }
+}
+
+/* kernels.dmt_block (core/kernels.py:1155-1168) semantics on time-major
+ * input: out[i][t] = sum_c x[(t - d) mod n][c] for t < n (circular roll by
+ * +delay, kernels.roll_block :1059-1099), float64 sum, float32 store. */
+void orc_dmt_roll_f32(const float* in, const int32_t* delays, int64_t ndm, int64_t nchans,
+                      int64_t nsamps, float* out) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads)
+  for (int64_t i = 0; i < ndm; ++i) {
+    for (int64_t t = 0; t < nsamps; ++t) {
+      double s = 0.0;
+      for (int64_t c = 0; c < nchans; ++c) {
+        int64_t sh = delays[i * nchans + c] % nsamps;
+        if (sh < 0) sh += nsamps;
+        int64_t r = t - sh;
+        if (r < 0) r += nsamps;
+        s += (double)in[r * nchans + c];
+      }
+      out[i * nsamps + t] = (float)s;
+    }
+  }
+}
+
+/* Packed-input DM batch: unpack (R4) then the row-wise contract, processing
+ * DM rows in parallel.  `in` holds nsamps*nchans*nbits/8 bytes. */
+void orc_dmt_packed_i32(const uint8_t* in, int nbits, int big, const int32_t* delays, int64_t ndm,
+                        int64_t nchans, int64_t nsamps, int64_t nvalid, int32_t* out,
+                        int64_t out_stride) {
+  const int64_t nbytes = nsamps * nchans * nbits / 8;
+  uint8_t* un;
+  if (nbits == 8) {
+    un = (uint8_t*)in;
+  } else {
+    un = (uint8_t*)malloc((size_t)(nsamps * nchans));
+    orc_unpack(in, nbytes, nbits, big, un);
+  }
+  orc_dmt_u8_i32(un, delays, ndm, nchans, nsamps, nvalid, out, out_stride);
+  if (nbits != 8) free(un);
+}
+
+/* kernels.extract_bpass (core/kernels.py:281-292): bpass[c] += x[t][c],
+ * float32 accumulation in sample order (bit-exact restatement). */
+void orc_bandpass_f32(const float* in, int64_t nchans, int64_t nsamps, float* bpass) {
+  for (int64_t t = 0; t < nsamps; ++t)
+    for (int64_t c = 0; c < nchans; ++c) bpass[c] = bpass[c] + in[t * nchans + c];
+}
+void orc_bandpass_u8(const uint8_t* in, int64_t nchans, int64_t nsamps, float* bpass) {
+  for (int64_t t = 0; t < nsamps; ++t)
+    for (int64_t c = 0; c < nchans; ++c) bpass[c] = bpass[c] + (float)in[t * nchans + c];
+}
+
+/* kernels.extract_tim (core/kernels.py:255-278): tim[out_start+t] += sum_c x
+ * (float64 accumulator). */
+void orc_collapse_f32(const float* in, int64_t nchans, int64_t nsamps, float* tim,
+                      int64_t out_start) {
+  for (int64_t t = 0; t < nsamps; ++t) {
+    double s = 0.0;
+    for (int64_t c = 0; c < nchans; ++c) s += (double)in[t * nchans + c];
+    tim[out_start + t] = (float)((double)tim[out_start + t] + s);
+  }
+}
+
+/* kernels.remove_zerodm (core/kernels.py:465-505), float32 data:
+ * y = f32((f64(x) - zdm * f64(w_c)) + f64(b_c)), zdm = sum_c f64(x[t][c]). */
+void orc_zero_dm_f32(const float* in, float* out, int64_t nchans, int64_t nsamps,
+                     const float* bpass, const float* chanwts) {
+#pragma omp parallel for num_threads(g_threads)
+  for (int64_t t = 0; t < nsamps; ++t) {
+    double z = 0.0;
+    for (int64_t c = 0; c < nchans; ++c) z += (double)in[t * nchans + c];
+    for (int64_t c = 0; c < nchans; ++c) {
+      volatile double t1 = z * (double)chanwts[c];
+      volatile double t2 = (double)in[t * nchans + c] - t1;
+      out[t * nchans + c] = (float)(t2 + (double)bpass[c]);
+    }
+  }
+}
+
+/* kernels.downsample_1d_mean (core/kernels.py:176-204). */
+void orc_downsample_mean(const float* in, int64_t n, int factor, float* out) {
+  const int64_t m = n / factor;
+  for (int64_t i = 0; i < m; ++i) {
+    double s = 0.0;
+    for (int k = 0; k < factor; ++k) s += (double)in[i * factor + k];
+    out[i] = (float)(s / factor);
+  }
+}
+
+/* Boxcar matched-filter S/N of one row (TimeSeries.downsample + z-score +
+ * apply_boxcar, timeseries.py:107-132, :296-325; core/stats.py:418-477 with
+ * loc=mean, scale=std), all in float64:
+ *   y = downsample_1d_mean(x, f) (values rounded to float32 as the reference)
+ *   snr_w = max_t (sum_{k<w} y[t+k] - w*mean(y)) / (std(y) * sqrt(w)).
+ * Writes snr[fi*nwidths + wi] and the argmax t to idx (may be NULL). */
+void orc_boxcar_snr_row(const float* x, int64_t n, const int32_t* factors, int nfactors,
+                        const int32_t* widths, int nwidths, double* snr, int32_t* idx) {
+  float* y = (float*)malloc(sizeof(float) * (n > 0 ? n : 1));
+  double* pre = (double*)malloc(sizeof(double) * (n + 1));
+  for (int fi = 0; fi < nfactors; ++fi) {
+    const int f = factors[fi];
+    const int64_t m = n / f;
+    orc_downsample_mean(x, n, f, y);
+    double s = 0.0, ss = 0.0;
+    pre[0] = 0.0;
+    for (int64_t i = 0; i < m; ++i) {
+      s += (double)y[i];
+      pre[i + 1] = s;
+    }
+    const double mean = m > 0 ? s / (double)m : 0.0;
+    for (int64_t i = 0; i < m; ++i) {
+      const double dlt = (double)y[i] - mean;
+      ss += dlt * dlt;
+    }
+    double sd = m > 0 ? sqrt(ss / (double)m) : 0.0;
+    if (sd == 0.0) sd = 1.0;
+    for (int wi = 0; wi < nwidths; ++wi) {
+      const int w = widths[wi];
+      double best = -INFINITY;
+      int64_t bt = -1;
+      for (int64_t t = 0; t + w <= m; ++t) {
+        const double v = pre[t + w] - pre[t];
+        if (v > best) { best = v; bt = t; }
+      }
+      snr[fi * nwidths + wi] = bt < 0 ? NAN : (best - (double)w * mean) / (sd * sqrt((double)w));
+      if (idx) idx[fi * nwidths + wi] = (int32_t)bt;
+    }
+  }
+  free(y);
+  free(pre);
+}
+
+/* kernels.subband (core/kernels.py:379-401) with a zero-initialised output:
+ * out[t*nsub + chan_to_sub[c]] += in[(t + d_c)*nchans + c], t < nsamps - maxdelay. */
+void orc_subband_u8(const uint8_t* in, float* out, const int32_t* delays, const int32_t* chan_to_sub,
+                    int64_t maxdelay, int64_t nchans, int64_t nsub, int64_t nsamps) {
+  const int64_t nout = nsamps - maxdelay;
+  for (int64_t t = 0; t < nout; ++t) {
+    for (int64_t s = 0; s < nsub; ++s) out[t * nsub + s] = 0.f;
+    for (int64_t c = 0; c < nchans; ++c)
+      out[t * nsub + chan_to_sub[c]] += (float)in[wrap_neg(t + delays[c], nsamps) * nchans + c];
+  }
+}

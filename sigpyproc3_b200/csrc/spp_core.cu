@@ -1,0 +1,607 @@
+// libsppgpu core: error state, unpack (R4), single-DM dedispersion (R2) and
+// the DM-trial batch plan (R3).  Host code for the kernels in spp_dmt.cuh.
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "spp_common.cuh"
+#include "spp_dmt.cuh"
+
+namespace spp {
+
+static thread_local char g_err[1024] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return SPP_OK;
+  return fail(SPP_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+static inline bool valid_nbits(int nbits) {
+  return nbits == 1 || nbits == 2 || nbits == 4 || nbits == 8 || nbits == 32;
+}
+
+// ---------------------------------------------------------------------------
+// R4: standalone unpack (kernels.unpack{1,2,4}_8_{big,little})
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void k_unpack(const uint8_t* __restrict__ in, int64_t nbytes, int bitorder,
+                         uint8_t* __restrict__ out) {
+  constexpr int per = 8 / NB;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nbytes;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t b = in[i];
+#pragma unroll
+    for (int k = 0; k < per; ++k) out[i * per + k] = (uint8_t)field_of<NB>(b, k, bitorder);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// DMT kernel variants
+// ---------------------------------------------------------------------------
+struct Variant {
+  int nb, acc, R, DW, TW, SLAB, STAGES;
+  void (*fn)(const DmtArgs);
+  int single;  // 1: meant for one DM (time-split warps)
+};
+
+template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
+static Variant mk(int single) {
+  return Variant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt<NB, R, DW, TW, SLAB, STAGES, ACC>,
+                 single};
+}
+
+#define SPP_INT_VARIANTS(NB)                    \
+  mk<NB, 2, 8, 1, 64, 3, 0>(0), mk<NB, 1, 8, 1, 64, 3, 0>(0), mk<NB, 2, 4, 2, 64, 3, 0>(0), \
+      mk<NB, 1, 16, 1, 64, 3, 0>(0), mk<NB, 2, 1, 4, 64, 3, 0>(1), mk<NB, 1, 1, 4, 64, 3, 0>(1)
+
+static const std::vector<Variant>& variants() {
+  static const std::vector<Variant> v = {
+      SPP_INT_VARIANTS(1),
+      SPP_INT_VARIANTS(2),
+      SPP_INT_VARIANTS(4),
+      SPP_INT_VARIANTS(8),
+      mk<8, 4, 1, 8, 64, 3, 0>(1),
+      // float32 input, compensated fp32
+      mk<32, 8, 8, 1, 32, 2, SPP_ACC_KAHAN32>(0),
+      mk<32, 4, 8, 2, 32, 2, SPP_ACC_KAHAN32>(0),
+      mk<32, 8, 16, 1, 32, 2, SPP_ACC_KAHAN32>(0),
+      mk<32, 4, 1, 4, 32, 2, SPP_ACC_KAHAN32>(1),
+      mk<32, 2, 1, 4, 32, 2, SPP_ACC_KAHAN32>(1),
+      // float32 input, fp64 accumulator
+      mk<32, 8, 8, 1, 32, 2, SPP_ACC_F64>(0),
+      mk<32, 4, 8, 2, 32, 2, SPP_ACC_F64>(0),
+      mk<32, 4, 1, 4, 32, 2, SPP_ACC_F64>(1),
+      mk<32, 2, 1, 4, 32, 2, SPP_ACC_F64>(1),
+  };
+  return v;
+}
+
+static inline int spw_of(int nb) { return nb == 32 ? 1 : 32 / nb; }
+static inline int64_t tile_T(const Variant& v) {
+  return (int64_t)v.TW * 32 * v.R * spw_of(v.nb);
+}
+
+static int slot_words(const Variant& v, int32_t span) {
+  const int spw = spw_of(v.nb);
+  const int64_t w = tile_T(v) / spw + ceil_div(std::max<int32_t>(span, 0), spw) + 6 + v.R;
+  return (int)round_up(w, 4);
+}
+
+static int64_t smem_bytes(const Variant& v, int slot_w) {
+  return v.STAGES * dmt_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
+}
+
+static constexpr int64_t kMaxSmem = 227 * 1024;
+
+// Planar geometry for one execution.
+struct Geometry {
+  int spw;
+  int64_t halo;     // samples
+  int64_t pitch_w;  // words per channel row
+  int64_t bytes;    // nchans * pitch_w * 4
+  int64_t ntiles_t;
+  int64_t nvalid;
+};
+
+// omin/omax: range of the signed offsets applied to t (sign * delay).
+static Geometry geometry(const Variant& v, int64_t nchans, int64_t nsamps, int64_t nvalid,
+                         int32_t omin, int32_t omax, int slot_w) {
+  Geometry g{};
+  g.spw = spw_of(v.nb);
+  g.nvalid = nvalid;
+  g.halo = round_up(std::max<int64_t>(0, -(int64_t)omin), 4 * g.spw);
+  g.ntiles_t = ceil_div(std::max<int64_t>(nvalid, 1), tile_T(v));
+  const int64_t last = g.ntiles_t * tile_T(v) + std::max<int64_t>(0, omax) + g.halo;
+  g.pitch_w = round_up(ceil_div(last, g.spw) + slot_w + 8, 4);
+  g.bytes = nchans * g.pitch_w * 4;
+  (void)nsamps;
+  return g;
+}
+
+static int ensure_smem(const Variant& v, int64_t bytes) {
+  if (bytes > kMaxSmem)
+    return fail(SPP_ERR_UNSUPPORTED, "DM tile needs %lld B of shared memory (> %lld)",
+                (long long)bytes, (long long)kMaxSmem);
+  if (bytes > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(v.fn),
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute");
+  }
+  return SPP_OK;
+}
+
+static int launch_corner_turn(int nb, const void* in, int bitorder, int64_t nchans,
+                              int64_t nsamps, const Geometry& g, void* planar, cudaStream_t st,
+                              const double* zdm = nullptr, const float* chanwts = nullptr,
+                              const float* bpass = nullptr) {
+  if (nb == 32) {
+    dim3 grid((unsigned)ceil_div(nchans, 32),
+              (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, 32), 65535));
+    k_corner_turn_f32<<<grid, 256, 0, st>>>(static_cast<const float*>(in), nchans, nsamps,
+                                            g.halo, static_cast<float*>(planar), g.pitch_w,
+                                            zdm, chanwts, bpass);
+  } else {
+    dim3 grid((unsigned)ceil_div(nchans, kCtChans),
+              (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, kCtWords), 65535));
+    const uint8_t* raw = static_cast<const uint8_t*>(in);
+    uint32_t* pl = static_cast<uint32_t*>(planar);
+    switch (nb) {
+      case 1: k_corner_turn_int<1><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, g.halo, pl, g.pitch_w); break;
+      case 2: k_corner_turn_int<2><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, g.halo, pl, g.pitch_w); break;
+      case 4: k_corner_turn_int<4><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, g.halo, pl, g.pitch_w); break;
+      default: k_corner_turn_int<8><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, g.halo, pl, g.pitch_w); break;
+    }
+  }
+  return cuda_status(cudaGetLastError(), "corner turn launch");
+}
+
+static int launch_dmt(const Variant& v, const DmtArgs& a, int64_t ntiles_t, int64_t ndm,
+                      cudaStream_t st) {
+  const int64_t smem = smem_bytes(v, a.slot_w);
+  int rc = ensure_smem(v, smem);
+  if (rc) return rc;
+  dim3 grid((unsigned)ceil_div(ndm, v.DW), (unsigned)ntiles_t);
+  if (ntiles_t > 65535)
+    return fail(SPP_ERR_UNSUPPORTED, "too many time tiles (%lld)", (long long)ntiles_t);
+  const int threads = (v.DW * v.TW + 1) * 32;
+  v.fn<<<grid, threads, smem, st>>>(a);
+  return cuda_status(cudaGetLastError(), "dmt launch");
+}
+
+// Single-DM shape: the largest time tile that still yields >= 2 CTAs per SM
+// (148 SMs), else the smallest tile.  Shapes are the same for both float
+// accumulators, so the workspace size does not depend on `acc`.
+static int pick_single_variant(int nb, int acc, int64_t nvalid) {
+  const auto& vs = variants();
+  int best_big = -1, best_small = -1;
+  for (int i = 0; i < (int)vs.size(); ++i) {
+    const Variant& v = vs[i];
+    if (!v.single || v.nb != nb || (nb == 32 && v.acc != acc)) continue;
+    const int64_t T = tile_T(v);
+    if (ceil_div(nvalid, T) >= 296 && (best_big < 0 || T > tile_T(vs[best_big]))) best_big = i;
+    if (best_small < 0 || T < tile_T(vs[best_small])) best_small = i;
+  }
+  return best_big >= 0 ? best_big : best_small;
+}
+
+}  // namespace spp
+
+using namespace spp;
+
+// ---------------------------------------------------------------------------
+// extern "C" entry points
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* spp_last_error_string(void) { return g_err; }
+
+int spp_version(void) { return 10000; }
+
+int spp_status_read(const void* workspace, uint32_t* host_out, void* stream) {
+  if (!workspace || !host_out) return fail(SPP_ERR_ARG, "spp_status_read: null pointer");
+  cudaStream_t st = as_stream(stream);
+  int rc = cuda_status(cudaMemcpyAsync(host_out, workspace, 16, cudaMemcpyDeviceToHost, st),
+                       "status copy");
+  if (rc) return rc;
+  rc = cuda_status(cudaStreamSynchronize(st), "status sync");
+  if (rc) return rc;
+  if (host_out[0] != 0)
+    return fail(SPP_ERR_DEVICE, "device status 0x%x (block %u, detail 0x%x)", host_out[0],
+                host_out[1], host_out[2]);
+  return SPP_OK;
+}
+
+int spp_status_clear(void* workspace, void* stream) {
+  if (!workspace) return fail(SPP_ERR_ARG, "spp_status_clear: null pointer");
+  return cuda_status(cudaMemsetAsync(workspace, 0, 16, as_stream(stream)), "status clear");
+}
+
+int spp_unpack(const uint8_t* in, int64_t nbytes, int nbits, int bitorder, uint8_t* out,
+               void* stream) {
+  if (nbytes < 0) return fail(SPP_ERR_ARG, "nbytes < 0");
+  if (nbytes == 0) return SPP_OK;
+  if (!in || !out) return fail(SPP_ERR_ARG, "spp_unpack: null pointer");
+  if (bitorder != SPP_BITORDER_BIG && bitorder != SPP_BITORDER_LITTLE)
+    return fail(SPP_ERR_ARG, "bad bitorder %d", bitorder);
+  cudaStream_t st = as_stream(stream);
+  const int threads = 256;
+  const int64_t blocks = std::min<int64_t>(ceil_div(nbytes, threads), 148 * 32);
+  switch (nbits) {
+    case 1: k_unpack<1><<<(unsigned)blocks, threads, 0, st>>>(in, nbytes, bitorder, out); break;
+    case 2: k_unpack<2><<<(unsigned)blocks, threads, 0, st>>>(in, nbytes, bitorder, out); break;
+    case 4: k_unpack<4><<<(unsigned)blocks, threads, 0, st>>>(in, nbytes, bitorder, out); break;
+    default: return fail(SPP_ERR_ARG, "unpack: nbits must be 1, 2 or 4 (got %d)", nbits);
+  }
+  return cuda_status(cudaGetLastError(), "unpack launch");
+}
+
+// ---------------------------------------------------------------------------
+// R2: single DM
+// ---------------------------------------------------------------------------
+static int single_setup(int nbits, int64_t nchans, int64_t nsamps, int32_t dmin, int32_t dmax,
+                        int acc, const Variant** vout, Geometry* gout, int* slot_out) {
+  if (!valid_nbits(nbits)) return fail(SPP_ERR_ARG, "nbits must be 1, 2, 4, 8 or 32 (got %d)", nbits);
+  if (nchans <= 0 || nsamps < 0) return fail(SPP_ERR_ARG, "bad shape nchans=%lld nsamps=%lld", (long long)nchans, (long long)nsamps);
+  if (nbits < 8 && (nchans * nbits) % 8 != 0)
+    return fail(SPP_ERR_ARG, "nchans*nbits must be a multiple of 8");
+  if (dmin > dmax) return fail(SPP_ERR_ARG, "delay_min > delay_max");
+  if (nchans > INT32_MAX) return fail(SPP_ERR_ARG, "nchans too large");
+  const int64_t maxabs = std::max<int64_t>(std::llabs(dmin), std::llabs(dmax));
+  const int64_t nvalid = nsamps - maxabs;
+  const int vi = pick_single_variant(nbits, acc, std::max<int64_t>(nvalid, 1));
+  if (vi < 0) return fail(SPP_ERR_UNSUPPORTED, "no kernel for nbits=%d acc=%d", nbits, acc);
+  const Variant& v = variants()[vi];
+  const int slot = slot_words(v, 0);
+  *vout = &v;
+  *slot_out = slot;
+  *gout = geometry(v, nchans, nsamps, nvalid, dmin, dmax, slot);
+  return SPP_OK;
+}
+
+int64_t spp_dedisperse_workspace_bytes(int nbits, int64_t nchans, int64_t nsamps,
+                                       int32_t delay_min, int32_t delay_max) {
+  const Variant* v;
+  Geometry g;
+  int slot;
+  if (single_setup(nbits, nchans, nsamps, delay_min, delay_max, SPP_ACC_F64, &v, &g, &slot))
+    return -1;
+  return kStatusBytes + g.bytes;
+}
+
+int spp_dedisperse(const void* in, int nbits, int bitorder, int64_t nchans, int64_t nsamps,
+                   const int32_t* delays, int32_t delay_min, int32_t delay_max, float* out,
+                   int64_t out_len, int64_t out_start, int acc, void* workspace,
+                   int64_t workspace_bytes, void* stream) {
+  if (!in || !delays || !out || !workspace) return fail(SPP_ERR_ARG, "spp_dedisperse: null pointer");
+  if (acc != SPP_ACC_F64 && acc != SPP_ACC_KAHAN32) return fail(SPP_ERR_ARG, "bad acc %d", acc);
+  const Variant* v;
+  Geometry g;
+  int slot;
+  int rc = single_setup(nbits, nchans, nsamps, delay_min, delay_max, acc, &v, &g, &slot);
+  if (rc) return rc;
+  if (g.nvalid <= 0) return SPP_OK;  // reference: prange over a non-positive count
+  if (-(int64_t)delay_min > nsamps)
+    return fail(SPP_ERR_DELAY, "negative delay %d reaches before the block", delay_min);
+  if (out_start < 0 || out_start + g.nvalid > out_len)
+    return fail(SPP_ERR_SIZE, "output too small: out_start %lld + %lld samples > out_len %lld",
+                (long long)out_start, (long long)g.nvalid, (long long)out_len);
+  if (workspace_bytes < kStatusBytes + g.bytes)
+    return fail(SPP_ERR_SIZE, "workspace %lld B < required %lld B", (long long)workspace_bytes,
+                (long long)(kStatusBytes + g.bytes));
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+    return fail(SPP_ERR_ALIGN, "workspace must be 256-B aligned");
+  cudaStream_t st = as_stream(stream);
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  void* planar = ws + kStatusBytes;
+  rc = launch_corner_turn(nbits, in, bitorder, nchans, nsamps, g, planar, st);
+  if (rc) return rc;
+  DmtArgs a{};
+  a.planar = planar;
+  a.pitch_w = g.pitch_w;
+  a.halo = g.halo;
+  a.nchans = (int32_t)nchans;
+  a.delays = delays;
+  a.dpitch = nchans;
+  a.ndm = 1;
+  a.sign = 1;
+  a.dlo = delay_min;
+  a.dhi = delay_max;
+  a.span_max = 0;
+  a.slot_w = slot;
+  a.out = out;
+  a.out_kind = SPP_OUT_F32;
+  a.out_stride = 0;
+  a.out_start = out_start;
+  a.nvalid = g.nvalid;
+  a.status = reinterpret_cast<uint32_t*>(ws);
+  return launch_dmt(*v, a, g.ntiles_t, 1, st);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// R3: DM-trial batch plan
+// ---------------------------------------------------------------------------
+struct spp_dmt_plan {
+  int nbits, bitorder, mode, out_kind, acc;
+  int64_t nchans, nsamps_max, ndm;
+  int32_t* d_delays = nullptr;  // device, ndm x dpitch (raw delays)
+  int64_t dpitch;
+  int32_t dmin, dmax;  // raw delay range
+  int32_t omin, omax;  // range of sign * delay
+  int32_t maxabs;
+  std::vector<int> cands;      // candidate variant indices
+  std::vector<int32_t> spans;  // span per candidate
+  int cur = 0;                 // index into cands
+};
+
+static int plan_sign(const spp_dmt_plan* p) { return p->mode == SPP_MODE_ROLL ? -1 : 1; }
+
+static int64_t plan_nvalid(const spp_dmt_plan* p, int64_t nsamps) {
+  return p->mode == SPP_MODE_ROLL ? nsamps : nsamps - p->maxabs;
+}
+
+extern "C" {
+
+int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nchans,
+                        int64_t nsamps_max, int64_t ndm, const int32_t* delays_host, int mode,
+                        int out_kind, int acc) {
+  if (!plan || !delays_host) return fail(SPP_ERR_ARG, "spp_dmt_plan_create: null pointer");
+  *plan = nullptr;
+  if (!valid_nbits(nbits)) return fail(SPP_ERR_ARG, "nbits must be 1, 2, 4, 8 or 32 (got %d)", nbits);
+  if (nchans <= 0 || ndm <= 0 || nsamps_max <= 0 || nchans > INT32_MAX || ndm > INT32_MAX)
+    return fail(SPP_ERR_ARG, "bad shape");
+  if (nbits < 8 && (nchans * nbits) % 8 != 0)
+    return fail(SPP_ERR_ARG, "nchans*nbits must be a multiple of 8");
+  if (mode != SPP_MODE_DEDISPERSE && mode != SPP_MODE_ROLL) return fail(SPP_ERR_ARG, "bad mode");
+  if (out_kind != SPP_OUT_F32 && out_kind != SPP_OUT_I32) return fail(SPP_ERR_ARG, "bad out_kind");
+  if (out_kind == SPP_OUT_I32 && nbits == 32)
+    return fail(SPP_ERR_ARG, "int32 output needs integer input");
+  if (acc != SPP_ACC_F64 && acc != SPP_ACC_KAHAN32) return fail(SPP_ERR_ARG, "bad acc");
+  if (bitorder != SPP_BITORDER_BIG && bitorder != SPP_BITORDER_LITTLE)
+    return fail(SPP_ERR_ARG, "bad bitorder");
+  spp_dmt_plan* p = new (std::nothrow) spp_dmt_plan();
+  if (!p) return fail(SPP_ERR_ARG, "out of host memory");
+  p->nbits = nbits; p->bitorder = bitorder; p->mode = mode; p->out_kind = out_kind; p->acc = acc;
+  p->nchans = nchans; p->nsamps_max = nsamps_max; p->ndm = ndm;
+  int32_t dmin = INT32_MAX, dmax = INT32_MIN;
+  for (int64_t i = 0; i < ndm * nchans; ++i) {
+    dmin = std::min(dmin, delays_host[i]);
+    dmax = std::max(dmax, delays_host[i]);
+  }
+  p->dmin = dmin; p->dmax = dmax;
+  p->maxabs = (int32_t)std::max<int64_t>(std::llabs(dmin), std::llabs(dmax));
+  const int sign = plan_sign(p);
+  p->omin = sign > 0 ? dmin : -dmax;
+  p->omax = sign > 0 ? dmax : -dmin;
+  if (mode == SPP_MODE_ROLL && p->maxabs >= nsamps_max) {
+    delete p;
+    return fail(SPP_ERR_DELAY, "roll mode needs |delay| < nsamps");
+  }
+  // candidates
+  const auto& vs = variants();
+  for (int i = 0; i < (int)vs.size(); ++i) {
+    const Variant& v = vs[i];
+    if (v.nb != nbits || (nbits == 32 && v.acc != acc)) continue;
+    if (ndm == 1 ? !v.single : v.single) continue;
+    // span for tiles of v.DW consecutive DMs
+    int32_t span = 0;
+    for (int64_t d0 = 0; d0 < ndm; d0 += v.DW) {
+      const int64_t d1 = std::min<int64_t>(ndm, d0 + v.DW);
+      for (int64_t c = 0; c < nchans; ++c) {
+        int32_t mn = INT32_MAX, mx = INT32_MIN;
+        for (int64_t d = d0; d < d1; ++d) {
+          const int32_t x = delays_host[d * nchans + c];
+          mn = std::min(mn, x);
+          mx = std::max(mx, x);
+        }
+        span = std::max(span, mx - mn);
+      }
+    }
+    if (smem_bytes(v, slot_words(v, span)) > kMaxSmem) continue;
+    p->cands.push_back(i);
+    p->spans.push_back(span);
+  }
+  if (p->cands.empty()) {
+    delete p;
+    return fail(SPP_ERR_UNSUPPORTED, "no kernel variant fits this delay table");
+  }
+  p->dpitch = nchans;
+  cudaError_t e = cudaMalloc(&p->d_delays, sizeof(int32_t) * ndm * nchans);
+  if (e != cudaSuccess) { delete p; return cuda_status(e, "plan cudaMalloc"); }
+  e = cudaMemcpy(p->d_delays, delays_host, sizeof(int32_t) * ndm * nchans, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { cudaFree(p->d_delays); delete p; return cuda_status(e, "plan upload"); }
+  *plan = p;
+  return SPP_OK;
+}
+
+int spp_dmt_plan_destroy(spp_dmt_plan* p) {
+  if (!p) return SPP_OK;
+  int rc = SPP_OK;
+  if (p->d_delays) rc = cuda_status(cudaFree(p->d_delays), "plan cudaFree");
+  delete p;
+  return rc;
+}
+
+int64_t spp_dmt_plan_nvalid(const spp_dmt_plan* p, int64_t nsamps) {
+  if (!p) return -1;
+  return std::max<int64_t>(0, plan_nvalid(p, nsamps));
+}
+
+int spp_dmt_plan_num_variants(const spp_dmt_plan* p) { return p ? (int)p->cands.size() : 0; }
+
+int spp_dmt_plan_set_variant(spp_dmt_plan* p, int variant) {
+  if (!p) return fail(SPP_ERR_ARG, "null plan");
+  if (variant < 0 || variant >= (int)p->cands.size()) return fail(SPP_ERR_ARG, "bad variant %d", variant);
+  p->cur = variant;
+  return SPP_OK;
+}
+
+int spp_dmt_plan_describe(const spp_dmt_plan* p, int32_t* cfg) {
+  if (!p || !cfg) return fail(SPP_ERR_ARG, "null pointer");
+  const Variant& v = variants()[p->cands[p->cur]];
+  const int slot = slot_words(v, p->spans[p->cur]);
+  cfg[0] = v.nb; cfg[1] = v.R; cfg[2] = v.DW; cfg[3] = v.TW; cfg[4] = v.SLAB; cfg[5] = v.STAGES;
+  cfg[6] = (int32_t)tile_T(v);
+  cfg[7] = (int32_t)smem_bytes(v, slot);
+  return SPP_OK;
+}
+
+static Geometry plan_geometry(const spp_dmt_plan* p, int64_t nsamps, int* slot) {
+  const Variant& v = variants()[p->cands[p->cur]];
+  *slot = slot_words(v, p->spans[p->cur]);
+  return geometry(v, p->nchans, nsamps, plan_nvalid(p, nsamps), p->omin, p->omax, *slot);
+}
+
+int64_t spp_dmt_plan_workspace_bytes(const spp_dmt_plan* p, int64_t nsamps) {
+  if (!p) return -1;
+  int slot;
+  Geometry g = plan_geometry(p, nsamps, &slot);
+  return kStatusBytes + g.bytes;
+}
+
+static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* out,
+                   int64_t out_stride, int64_t out_start, uint8_t* ws, int64_t ws_bytes,
+                   cudaStream_t st) {
+  int slot;
+  Geometry g = plan_geometry(p, nsamps, &slot);
+  if (g.nvalid <= 0) return SPP_OK;
+  if (p->mode == SPP_MODE_ROLL && p->maxabs >= nsamps)
+    return fail(SPP_ERR_DELAY, "roll mode needs |delay| < nsamps");
+  if (-(int64_t)p->omin > nsamps)
+    return fail(SPP_ERR_DELAY, "negative offset %d reaches before the block", p->omin);
+  if (ws_bytes < kStatusBytes + g.bytes)
+    return fail(SPP_ERR_SIZE, "workspace %lld B < required %lld B", (long long)ws_bytes,
+                (long long)(kStatusBytes + g.bytes));
+  if (out_start < 0 || (p->ndm > 1 && out_stride < out_start + g.nvalid))
+    return fail(SPP_ERR_SIZE, "out_stride %lld < out_start %lld + nvalid %lld",
+                (long long)out_stride, (long long)out_start, (long long)g.nvalid);
+  if (g.ntiles_t > 65535)
+    return fail(SPP_ERR_UNSUPPORTED, "%lld time tiles exceed the grid limit", (long long)g.ntiles_t);
+  const Variant& v = variants()[p->cands[p->cur]];
+  void* planar = ws + kStatusBytes;
+  int rc = launch_corner_turn(p->nbits, in, p->bitorder, p->nchans, nsamps, g, planar, st);
+  if (rc) return rc;
+  DmtArgs a{};
+  a.planar = planar;
+  a.pitch_w = g.pitch_w;
+  a.halo = g.halo;
+  a.nchans = (int32_t)p->nchans;
+  a.delays = p->d_delays;
+  a.dpitch = p->dpitch;
+  a.ndm = (int32_t)p->ndm;
+  a.sign = plan_sign(p);
+  a.dlo = p->omin;
+  a.dhi = p->omax;
+  a.span_max = p->spans[p->cur];
+  a.slot_w = slot;
+  a.out = out;
+  a.out_kind = p->out_kind;
+  a.out_stride = out_stride;
+  a.out_start = out_start;
+  a.nvalid = g.nvalid;
+  a.status = reinterpret_cast<uint32_t*>(ws);
+  return launch_dmt(v, a, g.ntiles_t, p->ndm, st);
+}
+
+int spp_dmt_execute(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* out,
+                    int64_t out_stride, int64_t out_start, void* workspace,
+                    int64_t workspace_bytes, void* stream) {
+  if (!p || !in || !out || !workspace) return fail(SPP_ERR_ARG, "spp_dmt_execute: null pointer");
+  if (nsamps <= 0 || nsamps > p->nsamps_max)
+    return fail(SPP_ERR_SIZE, "nsamps %lld outside (0, %lld]", (long long)nsamps, (long long)p->nsamps_max);
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+    return fail(SPP_ERR_ALIGN, "workspace must be 256-B aligned");
+  return dmt_run(p, in, nsamps, out, out_stride, out_start, static_cast<uint8_t*>(workspace),
+                 workspace_bytes, as_stream(stream));
+}
+
+// --- end-to-end from host buffers ------------------------------------------------
+static int64_t host_row_bytes(const spp_dmt_plan* p) {
+  return p->nbits == 32 ? p->nchans * 4 : p->nchans * p->nbits / 8;
+}
+
+struct HostLayout {
+  int64_t in_rows, in_bytes, out_bytes, run_bytes, set_bytes;
+};
+
+static HostLayout host_layout(const spp_dmt_plan* p, int64_t block) {
+  HostLayout h{};
+  h.in_rows = block + p->maxabs;
+  h.in_bytes = round_up(h.in_rows * host_row_bytes(p), 256);
+  h.out_bytes = round_up(p->ndm * block * 4, 256);
+  h.run_bytes = round_up(spp_dmt_plan_workspace_bytes(p, h.in_rows), 256);
+  h.set_bytes = h.in_bytes + h.out_bytes + h.run_bytes;
+  return h;
+}
+
+int64_t spp_dmt_host_workspace_bytes(const spp_dmt_plan* p, int64_t block_nsamps) {
+  if (!p || block_nsamps <= 0) return -1;
+  return kStatusBytes + 2 * host_layout(p, block_nsamps).set_bytes;
+}
+
+int spp_dmt_execute_host(const spp_dmt_plan* p, const void* in_host, int64_t nsamps,
+                         void* out_host, int64_t out_stride, int64_t block_nsamps,
+                         void* workspace, int64_t workspace_bytes) {
+  if (!p || !in_host || !out_host || !workspace) return fail(SPP_ERR_ARG, "null pointer");
+  if (p->mode != SPP_MODE_DEDISPERSE || p->omin < 0)
+    return fail(SPP_ERR_UNSUPPORTED, "host streaming needs dedisperse mode and delays >= 0");
+  if (block_nsamps <= 0) return fail(SPP_ERR_ARG, "block_nsamps <= 0");
+  const int64_t nvalid = plan_nvalid(p, nsamps);
+  if (nvalid <= 0) return SPP_OK;
+  if (out_stride < nvalid) return fail(SPP_ERR_SIZE, "out_stride < nvalid");
+  const HostLayout h = host_layout(p, block_nsamps);
+  if (h.in_rows > p->nsamps_max)
+    return fail(SPP_ERR_SIZE, "block + max delay (%lld) exceeds plan nsamps_max", (long long)h.in_rows);
+  if (workspace_bytes < kStatusBytes + 2 * h.set_bytes) return fail(SPP_ERR_SIZE, "workspace too small");
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return fail(SPP_ERR_ALIGN, "workspace must be 256-B aligned");
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  cudaStream_t s[2];
+  int rc = SPP_OK;
+  for (int i = 0; i < 2; ++i) {
+    rc = cuda_status(cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking), "stream create");
+    if (rc) { if (i) cudaStreamDestroy(s[0]); return rc; }
+  }
+  const int64_t rb = host_row_bytes(p);
+  const int64_t es = 4;
+  const int64_t nblocks = ceil_div(nvalid, block_nsamps);
+  for (int64_t b = 0; b < nblocks && rc == SPP_OK; ++b) {
+    const int k = (int)(b & 1);
+    uint8_t* set = ws + kStatusBytes + k * h.set_bytes;
+    uint8_t* d_in = set;
+    uint8_t* d_out = set + h.in_bytes;
+    uint8_t* d_run = set + h.in_bytes + h.out_bytes;
+    const int64_t t0 = b * block_nsamps;
+    const int64_t nout = std::min(block_nsamps, nvalid - t0);
+    const int64_t rows = nout + p->maxabs;
+    rc = cuda_status(cudaMemcpyAsync(d_in, static_cast<const uint8_t*>(in_host) + t0 * rb,
+                                     rows * rb, cudaMemcpyHostToDevice, s[k]), "H2D");
+    if (rc) break;
+    rc = dmt_run(p, d_in, rows, d_out, nout, 0, d_run, h.run_bytes, s[k]);
+    if (rc) break;
+    rc = cuda_status(cudaMemcpy2DAsync(static_cast<uint8_t*>(out_host) + t0 * es, out_stride * es,
+                                       d_out, nout * es, nout * es, p->ndm,
+                                       cudaMemcpyDeviceToHost, s[k]), "D2H");
+  }
+  for (int i = 0; i < 2; ++i) {
+    int r2 = cuda_status(cudaStreamSynchronize(s[i]), "stream sync");
+    if (!rc) rc = r2;
+    cudaStreamDestroy(s[i]);
+  }
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,471 @@
+// Brute-force DM-time transform kernels (device code, templates).
+//
+// Data path
+//   raw filterbank (time-major, nbits packed) --k_corner_turn--> "planar" rows
+//   (channel-major, time along 32-bit words, nbits per sample, LSB-first)
+//   --k_dmt--> out[dm][t] = sum_c planar[c][t + off(dm, c)]
+//
+// k_dmt: one CTA owns DW DM trials x T output samples.  It walks the channels
+// in slabs of SLAB channels.  A producer warp stages, per channel, the
+// 16-B-aligned window of that channel's planar row that the CTA's DMs touch
+// (cp.async.bulk, completion on an mbarrier, STAGES-deep ring); DW*TW
+// consumer warps each own one DM and 32*R words of time (R*spw samples per
+// thread) and accumulate with SIMD-within-a-register adds (integer input) or
+// compensated fp32 / fp64 (float input).  All waits are bounded.
+#pragma once
+
+#include "spp_common.cuh"
+
+namespace spp {
+
+// ----------------------------------------------------------------------------
+// Planar layout: row c holds samples s in [-halo, nsamps + pad) at word
+// (s + halo) / spw, bit ((s + halo) % spw) * NB.  halo is a multiple of 4*spw
+// samples so rows start 16-B aligned; pitch_w is a multiple of 4 words.
+// Samples outside [0, nsamps) wrap modulo nsamps (once), which reproduces
+// numba's negative-index wraparound used by kernels.dedisperse and the
+// circular roll of kernels.roll_block.
+// ----------------------------------------------------------------------------
+template <int NB>
+struct Pack {
+  static constexpr int kSpw = (NB == 32) ? 1 : 32 / NB;         // samples per word
+  static constexpr int kLogSpw = (NB == 32) ? 0 : (NB == 1 ? 5 : NB == 2 ? 4 : NB == 4 ? 3 : 2);
+  static constexpr uint32_t kMaskByte = (NB == 1)   ? 0x01010101u
+                                        : (NB == 2) ? 0x03030303u
+                                        : (NB == 4) ? 0x0F0F0F0Fu
+                                                    : 0xFFFFFFFFu;
+  static constexpr int kG = (NB >= 8) ? 1 : 8 / NB;  // samples per byte
+  // channels that fit in a byte lane / a 16-bit lane before overflow
+  static constexpr int kCap8 = (NB >= 8) ? 1 : 255 / ((1 << NB) - 1);
+  static constexpr int kCap16 = (NB >= 16) ? 1 : 65535 / ((1 << NB) - 1);
+};
+
+// Extracts the NB-bit field of channel `c` from its packed byte (sigproc
+// bit order: big = first channel in the most significant bits).
+template <int NB>
+__device__ __forceinline__ uint32_t field_of(uint32_t byte, int c, int bitorder) {
+  if (NB == 8) return byte;
+  constexpr int per = 8 / NB;
+  const int p = c % per;
+  const int sh = (bitorder == SPP_BITORDER_BIG) ? (8 - (p + 1) * NB) : (p * NB);
+  return (byte >> sh) & ((1u << NB) - 1u);
+}
+
+// Maps a planar sample index to a raw row index (wrap once) or -1 (zero).
+__device__ __forceinline__ int64_t wrap_row(int64_t s, int64_t nsamps) {
+  if (s < 0) s += nsamps;
+  else if (s >= nsamps) s -= nsamps;
+  return (s >= 0 && s < nsamps) ? s : -1;
+}
+
+// ----------------------------------------------------------------------------
+// Corner turn for packed integer data.  CTA = 64 channels x 16 planar words.
+// Loads the raw rows (16*spw of them, wrapped) of its channel group into
+// shared memory, builds one planar word per (channel, word) and writes rows
+// of 16 words.
+// ----------------------------------------------------------------------------
+constexpr int kCtChans = 64;
+constexpr int kCtWords = 16;
+
+template <int NB>
+__global__ void __launch_bounds__(256)
+k_corner_turn_int(const uint8_t* __restrict__ raw, int64_t nchans, int64_t nsamps,
+                  int bitorder, int64_t halo, uint32_t* __restrict__ planar,
+                  int64_t pitch_w) {
+  using P = Pack<NB>;
+  constexpr int RT = kCtWords * P::kSpw;      // raw rows in the tile
+  constexpr int SB = kCtChans * NB / 8;       // bytes per raw row segment (full tile)
+  constexpr int SBP = SB + 4;                 // smem pitch
+  __shared__ __align__(16) uint8_t s_raw[RT * SBP];
+  __shared__ uint32_t s_out[kCtChans][kCtWords + 1];
+
+  const int64_t c0 = (int64_t)blockIdx.x * kCtChans;
+  const int nc = (int)((nchans - c0) < kCtChans ? (nchans - c0) : kCtChans);
+  const int seg = (nc * NB + 7) / 8;
+  const int64_t rowbytes = nchans * NB / 8;
+  const int64_t segstart = c0 * NB / 8;
+  const bool vec = ((rowbytes & 3) == 0) && ((segstart & 3) == 0) && ((seg & 3) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(raw) & 3) == 0);
+  const int64_t ntw = (pitch_w + kCtWords - 1) / kCtWords;
+
+  for (int64_t by = blockIdx.y; by < ntw; by += gridDim.y) {
+    const int64_t w0 = by * kCtWords;
+    // load the raw rows of this tile (wrapped once around the block)
+    if (vec) {
+      const int nw = seg >> 2;
+      for (int idx = threadIdx.x; idx < RT * nw; idx += blockDim.x) {
+        const int r = idx / nw, k = idx - r * nw;
+        const int64_t row = wrap_row(w0 * P::kSpw + r - halo, nsamps);
+        uint32_t v = 0;
+        if (row >= 0) v = __ldg(reinterpret_cast<const uint32_t*>(raw + row * rowbytes + segstart) + k);
+        *reinterpret_cast<uint32_t*>(s_raw + r * SBP + 4 * k) = v;
+      }
+    } else {
+      for (int idx = threadIdx.x; idx < RT * seg; idx += blockDim.x) {
+        const int r = idx / seg, k = idx - r * seg;
+        const int64_t row = wrap_row(w0 * P::kSpw + r - halo, nsamps);
+        s_raw[r * SBP + k] = (row >= 0) ? __ldg(raw + row * rowbytes + segstart + k) : 0;
+      }
+    }
+    __syncthreads();
+    // build planar words: lanes over channels (conflict-free byte reads)
+    for (int idx = threadIdx.x; idx < kCtChans * kCtWords; idx += blockDim.x) {
+      const int c = idx % kCtChans, w = idx / kCtChans;
+      uint32_t v = 0;
+      if (c < nc) {
+        const int byte = (c * NB) / 8;
+#pragma unroll
+        for (int j = 0; j < P::kSpw; ++j) {
+          const uint32_t b = s_raw[(w * P::kSpw + j) * SBP + byte];
+          v |= field_of<NB>(b, c, bitorder) << (j * NB);
+        }
+      }
+      s_out[c][w] = v;
+    }
+    __syncthreads();
+    // store rows (lanes over words)
+    for (int idx = threadIdx.x; idx < kCtChans * kCtWords; idx += blockDim.x) {
+      const int w = idx % kCtWords, c = idx / kCtWords;
+      if (c < nc && w0 + w < pitch_w) planar[(c0 + c) * pitch_w + w0 + w] = s_out[c][w];
+    }
+    __syncthreads();
+  }
+}
+
+// Corner turn for float32 data, optionally fused with zero-DM subtraction
+// (kernels.remove_zerodm, core/kernels.py:465-505):
+//   y = f32((f64(x) - zdm[t] * f64(chanwts[c])) + f64(bpass[c]))
+// computed with round-to-nearest intrinsics (no contraction).
+static __global__ void __launch_bounds__(256)
+k_corner_turn_f32(const float* __restrict__ raw, int64_t nchans, int64_t nsamps,
+                  int64_t halo, float* __restrict__ planar, int64_t pitch,
+                  const double* __restrict__ zdm, const float* __restrict__ chanwts,
+                  const float* __restrict__ bpass) {
+  __shared__ float tile[32][33];
+  const int64_t c0 = (int64_t)blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  const int64_t nty = (pitch + 31) / 32;
+  for (int64_t by = blockIdx.y; by < nty; by += gridDim.y) {
+    const int64_t p0 = by * 32;  // planar column (sample + halo)
+    for (int i = ty; i < 32; i += 8) {
+      const int64_t row = wrap_row(p0 + i - halo, nsamps);
+      const int64_t c = c0 + tx;
+      float v = 0.f;
+      if (row >= 0 && c < nchans) {
+        v = __ldg(raw + row * nchans + c);
+        if (zdm != nullptr) {
+          const double t1 = __dmul_rn(zdm[row], (double)chanwts[c]);
+          const double t2 = __dsub_rn((double)v, t1);
+          v = (float)__dadd_rn(t2, (double)bpass[c]);
+        }
+      }
+      tile[i][tx] = v;
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+      const int64_t c = c0 + i;
+      const int64_t p = p0 + tx;
+      if (c < nchans && p < pitch) planar[c * pitch + p] = tile[tx][i];
+    }
+    __syncthreads();
+  }
+}
+
+// Per-sample zero-DM sums zdm[t] = sum_c f64(x[t][c]) (one warp per sample).
+static __global__ void k_row_sum_f64(const float* __restrict__ raw, int64_t nchans, int64_t nsamps,
+                              double* __restrict__ zdm) {
+  const int64_t t = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (t >= nsamps) return;
+  double s = 0.0;
+  for (int64_t c = lane; c < nchans; c += 32) s += (double)__ldg(raw + t * nchans + c);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) zdm[t] = s;
+}
+
+// ----------------------------------------------------------------------------
+// Accumulators
+// ----------------------------------------------------------------------------
+// Integer NB in {1,2,4,8}: byte lanes (A) -> 16-bit lanes (E: bytes 0/2, O:
+// bytes 1/3) -> 32-bit per-sample sums (S).  Byte lane i of A[k][g] holds the
+// running sum of sample i*G + g of word k.
+template <int NB, int R>
+struct IntAcc {
+  using P = Pack<NB>;
+  static constexpr int G = P::kG;
+  static constexpr int SPW = P::kSpw;
+  uint32_t A[R][G];
+  uint32_t E[R][G];
+  uint32_t O[R][G];
+  uint32_t S[R][SPW];
+
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+#pragma unroll
+      for (int g = 0; g < G; ++g) A[k][g] = E[k][g] = O[k][g] = 0u;
+#pragma unroll
+      for (int j = 0; j < SPW; ++j) S[k][j] = 0u;
+    }
+  }
+  __device__ __forceinline__ void add(uint32_t v, int k) {
+    if (NB == 8) {
+      E[k][0] += v & 0x00FF00FFu;
+      O[k][0] += (v >> 8) & 0x00FF00FFu;
+    } else {
+#pragma unroll
+      for (int g = 0; g < G; ++g) A[k][g] += (v >> (g * NB)) & P::kMaskByte;
+    }
+  }
+  __device__ __forceinline__ void flush8() {
+    if (NB == 8) return;
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        E[k][g] += A[k][g] & 0x00FF00FFu;
+        O[k][g] += (A[k][g] >> 8) & 0x00FF00FFu;
+        A[k][g] = 0u;
+      }
+  }
+  __device__ __forceinline__ void flush16() {
+#pragma unroll
+    for (int k = 0; k < R; ++k)
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        S[k][0 * G + g] += E[k][g] & 0xFFFFu;
+        S[k][2 * G + g] += E[k][g] >> 16;
+        S[k][1 * G + g] += O[k][g] & 0xFFFFu;
+        S[k][3 * G + g] += O[k][g] >> 16;
+        E[k][g] = O[k][g] = 0u;
+      }
+  }
+};
+
+// ----------------------------------------------------------------------------
+// DM-time transform kernel
+// ----------------------------------------------------------------------------
+struct DmtArgs {
+  const void* planar;     // planar rows (uint32 words or floats)
+  int64_t pitch_w;        // row pitch in words
+  int64_t halo;           // samples of left halo
+  int32_t nchans;
+  const int32_t* delays;  // ndm x dpitch
+  int64_t dpitch;
+  int32_t ndm;
+  int32_t sign;           // +1 dedisperse, -1 roll
+  int32_t dlo, dhi;       // declared range of sign*delay
+  int32_t span_max;       // max (dmax - dmin) over a DM tile and channel
+  int32_t slot_w;         // words per channel per stage
+  void* out;
+  int32_t out_kind;
+  int64_t out_stride;
+  int64_t out_start;
+  int64_t nvalid;
+  uint32_t* status;
+};
+
+template <int NB, int R, int DW, int TW, int SLAB, int STAGES>
+struct DmtShape {
+  static constexpr int kSpw = Pack<NB>::kSpw;
+  static constexpr int kNwc = DW * TW;                 // consumer warps
+  static constexpr int kThreads = (kNwc + 1) * 32;     // + producer warp
+  static constexpr int kT = TW * 32 * R * kSpw;        // samples per CTA tile
+};
+
+__host__ __device__ constexpr int64_t dmt_stage_bytes(int slab, int slot_w, int dw) {
+  return (int64_t)slab * slot_w * 4 + (int64_t)dw * slab * 4 + (int64_t)slab * 4;
+}
+
+template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
+__global__ void __launch_bounds__(DmtShape<NB, R, DW, TW, SLAB, STAGES>::kThreads)
+k_dmt(const DmtArgs a) {
+  using Sh = DmtShape<NB, R, DW, TW, SLAB, STAGES>;
+  using P = Pack<NB>;
+  constexpr int SPW = P::kSpw;
+  constexpr int NWC = Sh::kNwc;
+  constexpr int T = Sh::kT;
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
+  int32_t* sdel = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * a.slot_w);
+  int32_t* sbase = sdel + STAGES * DW * SLAB;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sbase + STAGES * SLAB + ((STAGES * SLAB) & 1));
+  uint64_t* empty = full + STAGES;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int dm0 = blockIdx.x * DW;
+  const int64_t t0 = (int64_t)blockIdx.y * T;
+  const int nslab = (a.nchans + SLAB - 1) / SLAB;
+
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NWC);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == NWC) {
+    // ---------------- producer warp ----------------
+    const uint32_t* planar = static_cast<const uint32_t*>(a.planar);
+    for (int k = 0; k < nslab; ++k) {
+      const int s = k % STAGES;
+      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1, a.status)) break;
+      const int c0 = k * SLAB;
+      const int nc = min(SLAB, a.nchans - c0);
+      int64_t ws_reg[(SLAB + 31) / 32];
+#pragma unroll
+      for (int jj = 0; jj < (SLAB + 31) / 32; ++jj) {
+        const int j = lane + jj * 32;
+        ws_reg[jj] = 0;
+        if (j < nc) {
+          const int c = c0 + j;
+          int32_t dv[DW];
+          int32_t mn = INT32_MAX, mx = INT32_MIN;
+#pragma unroll
+          for (int i = 0; i < DW; ++i) {
+            const int dm = min(dm0 + i, a.ndm - 1);
+            int32_t d = a.sign * __ldg(a.delays + (int64_t)dm * a.dpitch + c);
+            if (d < a.dlo || d > a.dhi) {
+              dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)c);
+              d = min(max(d, a.dlo), a.dhi);
+            }
+            dv[i] = d;
+            mn = min(mn, d);
+            mx = max(mx, d);
+          }
+          if (mx - mn > a.span_max) {
+            dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)c | 0x80000000u);
+            mx = mn + a.span_max;
+          }
+#pragma unroll
+          for (int i = 0; i < DW; ++i)
+            sdel[(s * DW + i) * SLAB + j] = min(dv[i], mx);
+          const int64_t ws = ((t0 + mn + a.halo) / SPW) & ~int64_t(3);
+          sbase[s * SLAB + j] = (int32_t)(ws * SPW - a.halo - t0);
+          ws_reg[jj] = ws;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive_expect_tx(&full[s], (uint32_t)nc * a.slot_w * 4u);
+      __syncwarp();
+#pragma unroll
+      for (int jj = 0; jj < (SLAB + 31) / 32; ++jj) {
+        const int j = lane + jj * 32;
+        if (j < nc)
+          bulk_g2s(sdata + ((int64_t)s * SLAB + j) * a.slot_w,
+                   planar + (int64_t)(c0 + j) * a.pitch_w + ws_reg[jj], a.slot_w * 4u, &full[s]);
+      }
+    }
+    return;
+  }
+
+  // ---------------- consumer warps ----------------
+  const int dmw = warp / TW, tw = warp % TW;
+  const int dm = dm0 + dmw;
+  const int tloc = tw * (32 * R * SPW) + lane * (R * SPW);
+  bool ok = true;
+
+  if constexpr (NB == 32) {
+    // float32 input
+    float s_acc[R], c_acc[R];
+    double d_acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) { s_acc[r] = 0.f; c_acc[r] = 0.f; d_acc[r] = 0.0; }
+    for (int k = 0; k < nslab; ++k) {
+      const int s = k % STAGES;
+      if (!mbar_wait(&full[s], (k / STAGES) & 1, a.status)) { ok = false; break; }
+      const int nc = min(SLAB, a.nchans - k * SLAB);
+      const float* sd = reinterpret_cast<const float*>(sdata) + (int64_t)s * SLAB * a.slot_w;
+      const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
+      const int32_t* bs = sbase + s * SLAB;
+#pragma unroll 4
+      for (int j = 0; j < nc; ++j) {
+        const float* row = sd + j * a.slot_w + (tloc + dl[j] - bs[j]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float x = row[r];
+          if (ACC == SPP_ACC_F64) {
+            d_acc[r] += (double)x;
+          } else {
+            const float y = __fsub_rn(x, c_acc[r]);
+            const float t = __fadd_rn(s_acc[r], y);
+            c_acc[r] = __fsub_rn(__fsub_rn(t, s_acc[r]), y);
+            s_acc[r] = t;
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+    if (!ok || dm >= a.ndm) return;
+    float* out = static_cast<float*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t t = t0 + tloc + r;
+      if (t < a.nvalid)
+        out[t] = (ACC == SPP_ACC_F64) ? (float)d_acc[r] : __fsub_rn(s_acc[r], c_acc[r]);
+    }
+  } else {
+    IntAcc<NB, R> acc;
+    acc.zero();
+    constexpr int K16 = (P::kCap16 / SLAB) > 0 ? (P::kCap16 / SLAB) : 1;
+    constexpr int F8 = (P::kCap8 >= SLAB) ? SLAB : 16;  // byte-lane flush period (channels)
+    static_assert(NB == 8 || P::kCap8 >= F8, "byte lanes would overflow");
+    static_assert(NB != 8 || P::kCap16 >= SLAB, "16-bit lanes would overflow");
+    for (int k = 0; k < nslab; ++k) {
+      const int s = k % STAGES;
+      if (!mbar_wait(&full[s], (k / STAGES) & 1, a.status)) { ok = false; break; }
+      const int nc = min(SLAB, a.nchans - k * SLAB);
+      const uint32_t* sd = sdata + (int64_t)s * SLAB * a.slot_w;
+      const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
+      const int32_t* bs = sbase + s * SLAB;
+      for (int jb = 0; jb < nc; jb += F8) {
+        const int je = min(nc, jb + F8);
+#pragma unroll 4
+        for (int j = jb; j < je; ++j) {
+          const int o = tloc + dl[j] - bs[j];
+          const uint32_t* row = sd + j * a.slot_w + (o >> P::kLogSpw);
+          const int sh = (o & (SPW - 1)) * NB;
+          uint32_t w[R + 1];
+#pragma unroll
+          for (int r = 0; r <= R; ++r) w[r] = row[r];
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc.add(__funnelshift_r(w[r], w[r + 1], sh), r);
+        }
+        acc.flush8();
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+      if (((k + 1) % K16) == 0) acc.flush16();
+    }
+    acc.flush16();
+    if (!ok || dm >= a.ndm) return;
+    const int64_t tb = t0 + tloc;
+    if (a.out_kind == SPP_OUT_I32) {
+      int32_t* out = static_cast<int32_t*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int j = 0; j < SPW; ++j) {
+          const int64_t t = tb + r * SPW + j;
+          if (t < a.nvalid) out[t] = (int32_t)acc.S[r][j];
+        }
+    } else {
+      float* out = static_cast<float*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int j = 0; j < SPW; ++j) {
+          const int64_t t = tb + r * SPW + j;
+          if (t < a.nvalid) out[t] = (float)acc.S[r][j];
+        }
+    }
+  }
+}
+
+}  // namespace spp

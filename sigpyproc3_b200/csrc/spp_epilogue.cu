@@ -1,0 +1,508 @@
+// Channel reductions (bandpass, collapse), zero-DM, downsample, stage-1
+// subband, and the boxcar matched-filter S/N epilogue.
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+
+#include "spp_common.cuh"
+#include "spp_dmt.cuh"
+
+namespace spp {
+
+static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+__host__ __device__ __forceinline__ int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
+
+// Reads sample (t, c) of a raw time-major block as float (any nbits).
+template <int NB>
+__device__ __forceinline__ float raw_at(const void* in, int64_t nchans, int64_t t, int64_t c,
+                                        int bitorder) {
+  if (NB == 32) return static_cast<const float*>(in)[t * nchans + c];
+  const uint8_t* b = static_cast<const uint8_t*>(in);
+  const int64_t bit = (t * nchans + c) * NB;
+  return (float)field_of<NB>(b[bit >> 3], (int)c, bitorder);
+}
+
+// ---------------------------------------------------------------------------
+// bandpass: per-channel sequential float32 sum over samples, in sample order,
+// exactly as kernels.extract_bpass's loop (bit-identical).  One thread per
+// channel; 8 samples are loaded ahead of the dependent add chain.
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void k_bandpass(const void* __restrict__ in, int64_t nchans, int64_t nsamps,
+                           int bitorder, float* __restrict__ bpass) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchans) return;
+  float acc = bpass[c];
+  int64_t t = 0;
+  for (; t + 8 <= nsamps; t += 8) {
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = raw_at<NB>(in, nchans, t + k, c, bitorder);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc = __fadd_rn(acc, v[k]);
+  }
+  for (; t < nsamps; ++t) acc = __fadd_rn(acc, raw_at<NB>(in, nchans, t, c, bitorder));
+  bpass[c] = acc;
+}
+
+// collapse: tim[out_start + t] = f32(sum_c f64(x[t][c])) (kernels.extract_tim)
+template <int NB>
+__global__ void k_collapse(const void* __restrict__ in, int64_t nchans, int64_t nsamps,
+                           int bitorder, float* __restrict__ tim, int64_t out_start) {
+  const int64_t t = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (t >= nsamps) return;
+  double s = 0.0;
+  for (int64_t c = lane; c < nchans; c += 32) s += (double)raw_at<NB>(in, nchans, t, c, bitorder);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) tim[out_start + t] = (float)s;
+}
+
+// zero-DM on time-major float32 (kernels.remove_zerodm): one block per sample.
+__global__ void k_zero_dm(const float* __restrict__ in, float* __restrict__ out, int64_t nchans,
+                          int64_t nsamps, const float* __restrict__ bpass,
+                          const float* __restrict__ chanwts) {
+  __shared__ double red[32];
+  for (int64_t t = blockIdx.x; t < nsamps; t += gridDim.x) {
+    double s = 0.0;
+    for (int64_t c = threadIdx.x; c < nchans; c += blockDim.x) s += (double)in[t * nchans + c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (threadIdx.x == 0) red[0] = v;
+    }
+    __syncthreads();
+    const double z = red[0];
+    for (int64_t c = threadIdx.x; c < nchans; c += blockDim.x) {
+      const double t1 = __dmul_rn(z, (double)chanwts[c]);
+      const double t2 = __dsub_rn((double)in[t * nchans + c], t1);
+      out[t * nchans + c] = (float)__dadd_rn(t2, (double)bpass[c]);
+    }
+    __syncthreads();
+  }
+}
+
+// downsample_1d_mean over rows
+__global__ void k_downsample(const float* __restrict__ in, int64_t n, int64_t in_stride,
+                             int factor, float* __restrict__ out, int64_t out_stride) {
+  const int64_t m = n / factor;
+  const int64_t row = blockIdx.y;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < factor; ++k) s += (double)in[row * in_stride + i * factor + k];
+    out[row * out_stride + i] = (float)(s / factor);
+  }
+}
+
+// downsample_2d_mean_flat
+__global__ void k_downsample_2d(const float* __restrict__ in, int64_t dim1, int64_t dim2,
+                                int f1, int f2, float* __restrict__ out) {
+  const int64_t n1 = dim1 / f1, n2 = dim2 / f2;
+  const int64_t total = n1 * n2;
+  const double tot = (double)f1 * f2;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = idx / n2, j = idx - i * n2;
+    double s = 0.0;
+    const int64_t pos = dim2 * i * f1 + j * f2;
+    for (int a = 0; a < f1; ++a)
+      for (int b = 0; b < f2; ++b) s += (double)in[pos + a * dim2 + b];
+    out[idx] = (float)(s / tot);
+  }
+}
+
+// stage-1 subband (kernels.subband with a zeroed output): atomics into
+// out[t][sub], exact for integer input (sums < 2^24).
+template <int NB>
+__global__ void k_subband(const void* __restrict__ in, int64_t nchans, int64_t nsamps,
+                          int bitorder, const int32_t* __restrict__ delays,
+                          const int32_t* __restrict__ chan_to_sub, int64_t nsub, int64_t nout,
+                          float* __restrict__ out) {
+  const int64_t total = nout * nchans;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t t = idx / nchans, c = idx - t * nchans;
+    int64_t r = t + delays[c];
+    if (r < 0) r += nsamps;
+    if (r < 0 || r >= nsamps) continue;
+    const int s = chan_to_sub[c];
+    if (s < 0 || s >= nsub) continue;
+    atomicAdd(out + t * nsub + s, raw_at<NB>(in, nchans, r, c, bitorder));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Boxcar S/N.  Chunk pass: CTA (chunk k, row r, factor fi) builds the
+// downsampled series y over its chunk plus a halo of (wmax-1) samples in
+// shared memory as float64, scans it to prefix sums, and records per width the
+// best window sum starting inside the chunk (smallest start on ties) plus the
+// chunk's sum and second central moment.  Final pass merges chunks (Chan et
+// al. 1979 pairwise variance) and forms (best - w*mean) / (std*sqrt(w)).
+// ---------------------------------------------------------------------------
+constexpr int kSnrChunk = 4096;
+constexpr int kSnrThreads = 512;
+constexpr int kSnrMaxW = 4096;
+constexpr int kSnrMaxWidths = 32;
+
+struct SnrPart {
+  double best;
+  int64_t idx;
+};
+
+struct SnrCfg {
+  int nf, nw, wmax;
+  int32_t f[8];
+  int32_t w[kSnrMaxWidths];
+};
+
+__device__ __forceinline__ double row_val(const void* in, int kind, int64_t i) {
+  return kind == SPP_OUT_I32 ? (double)static_cast<const int32_t*>(in)[i]
+                             : (double)static_cast<const float*>(in)[i];
+}
+
+__global__ void __launch_bounds__(kSnrThreads)
+k_snr_chunk(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride, const SnrCfg cfg,
+            int64_t nchunks, SnrPart* __restrict__ parts, double* __restrict__ stats) {
+  const int nfactors = cfg.nf, nwidths = cfg.nw, wmax = cfg.wmax;
+  extern __shared__ double sy[];  // kSnrChunk + wmax + 1
+  __shared__ double red_d[kSnrThreads / 32];
+  __shared__ long long red_i[kSnrThreads / 32];
+  __shared__ double carry;
+  const int64_t k = blockIdx.x;
+  const int64_t row = blockIdx.y / nfactors;
+  const int fi = blockIdx.y % nfactors;
+  const int f = cfg.f[fi];
+  const int64_t m = n / f;
+  const int64_t i0 = k * kSnrChunk;
+  if (i0 >= m) {
+    return;
+  }
+  const int64_t own = imin64(kSnrChunk, m - i0);
+  const int64_t len = imin64(own + wmax, m - i0);  // samples loaded
+  const char* base = static_cast<const char*>(in) + row * in_stride * 4;
+  // y values (downsampled means rounded to float32 as the reference output dtype)
+  for (int64_t j = threadIdx.x; j < len; j += blockDim.x) {
+    double s = 0.0;
+    const int64_t x0 = (i0 + j) * f;
+    for (int q = 0; q < f; ++q) s += row_val(base, kind, x0 + q);
+    sy[j + 1] = (double)(float)(s / f);
+  }
+  if (threadIdx.x == 0) { sy[0] = 0.0; carry = 0.0; }
+  __syncthreads();
+  // chunk sum and M2 over owned samples
+  {
+    double s = 0.0;
+    for (int64_t j = threadIdx.x; j < own; j += blockDim.x) s += sy[j + 1];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red_d[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kSnrThreads / 32; ++w) t += red_d[w];
+      carry = t;
+    }
+    __syncthreads();
+    const double mu = carry / (double)own;
+    double q = 0.0;
+    for (int64_t j = threadIdx.x; j < own; j += blockDim.x) {
+      const double d = sy[j + 1] - mu;
+      q += d * d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red_d[threadIdx.x >> 5] = q;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kSnrThreads / 32; ++w) t += red_d[w];
+      double* st = stats + ((row * nfactors + fi) * nchunks + k) * 3;
+      st[0] = (double)own;
+      st[1] = carry;
+      st[2] = t;
+    }
+    __syncthreads();
+  }
+  // inclusive scan of sy[1..len] (sequential per thread segment + warp/block scan)
+  {
+    const int64_t per = (len + blockDim.x - 1) / blockDim.x;
+    const int64_t a = 1 + threadIdx.x * per;
+    const int64_t b = imin64(a + per, len + 1);
+    double s = 0.0;
+    for (int64_t j = a; j < b; ++j) { s += sy[j]; sy[j] = s; }
+    // exclusive scan of segment totals across threads
+    double incl = s;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) red_d[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double acc = 0.0;
+      for (int w = 0; w < kSnrThreads / 32; ++w) { const double v = red_d[w]; red_d[w] = acc; acc += v; }
+    }
+    __syncthreads();
+    const double off = red_d[warp] + (incl - s);
+    for (int64_t j = a; j < b; ++j) sy[j] += off;
+    __syncthreads();
+  }
+  // window maxima per width
+  for (int wi = 0; wi < nwidths; ++wi) {
+    const int w = cfg.w[wi];
+    double best = -DBL_MAX;
+    long long bidx = LLONG_MAX;
+    for (int64_t t = threadIdx.x; t < own; t += blockDim.x) {
+      if (t + w > len) break;  // beyond the row end (len == m - i0 there)
+      const double v = sy[t + w] - sy[t];
+      if (v > best) { best = v; bidx = i0 + t; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+      const long long oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+      if (ov > best || (ov == best && oi < bidx)) { best = ov; bidx = oi; }
+    }
+    if ((threadIdx.x & 31) == 0) { red_d[threadIdx.x >> 5] = best; red_i[threadIdx.x >> 5] = bidx; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      best = red_d[0];
+      bidx = red_i[0];
+      for (int w2 = 1; w2 < kSnrThreads / 32; ++w2)
+        if (red_d[w2] > best || (red_d[w2] == best && red_i[w2] < bidx)) { best = red_d[w2]; bidx = red_i[w2]; }
+      SnrPart* p = parts + (((row * nfactors + fi) * nwidths + wi) * nchunks + k);
+      p->best = best;
+      p->idx = bidx;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_snr_final(int64_t n, const SnrCfg cfg, int64_t nrows, int64_t nchunks, const SnrPart* __restrict__ parts,
+                            const double* __restrict__ stats, float* __restrict__ snr,
+                            int32_t* __restrict__ peak) {
+  const int nfactors = cfg.nf, nwidths = cfg.nw;
+  const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= nrows * nfactors * nwidths) return;
+  const int wi = id % nwidths;
+  const int64_t rf = id / nwidths;  // row * nfactors + fi
+  const int fi = rf % nfactors;
+  const int64_t m = n / cfg.f[fi];
+  const int64_t nck = (m + kSnrChunk - 1) / kSnrChunk;
+  // merge moments
+  double cnt = 0.0, mean = 0.0, m2 = 0.0;
+  for (int64_t k = 0; k < nck; ++k) {
+    const double* st = stats + (rf * nchunks + k) * 3;
+    const double nb = st[0];
+    if (nb <= 0) continue;
+    const double mb = st[1] / nb;
+    const double d = mb - mean;
+    const double tot = cnt + nb;
+    mean += d * nb / tot;
+    m2 += st[2] + d * d * cnt * nb / tot;
+    cnt = tot;
+  }
+  double sd = cnt > 0 ? sqrt(m2 / cnt) : 0.0;
+  if (sd == 0.0) sd = 1.0;
+  double best = -DBL_MAX;
+  long long bidx = -1;
+  for (int64_t k = 0; k < nck; ++k) {
+    const SnrPart p = parts[(rf * nwidths + wi) * nchunks + k];
+    if (p.idx < 0 || p.idx == LLONG_MAX) continue;
+    if (p.best > best) { best = p.best; bidx = p.idx; }
+  }
+  const int w = cfg.w[wi];
+  snr[id] = bidx < 0 ? NAN : (float)((best - (double)w * mean) / (sd * sqrt((double)w)));
+  if (peak) peak[id] = (int32_t)bidx;
+}
+
+template <typename F>
+static int dispatch_nb(int nbits, F&& f) {
+  switch (nbits) {
+    case 1: f(std::integral_constant<int, 1>()); return SPP_OK;
+    case 2: f(std::integral_constant<int, 2>()); return SPP_OK;
+    case 4: f(std::integral_constant<int, 4>()); return SPP_OK;
+    case 8: f(std::integral_constant<int, 8>()); return SPP_OK;
+    case 32: f(std::integral_constant<int, 32>()); return SPP_OK;
+    default: return fail(SPP_ERR_ARG, "nbits must be 1, 2, 4, 8 or 32 (got %d)", nbits);
+  }
+}
+
+static int check_raw(const void* in, int nbits, int bitorder, int64_t nchans, int64_t nsamps) {
+  if (!in) return fail(SPP_ERR_ARG, "null input");
+  if (nchans <= 0 || nsamps < 0) return fail(SPP_ERR_ARG, "bad shape");
+  if (nbits < 8 && (nchans * nbits) % 8) return fail(SPP_ERR_ARG, "nchans*nbits must be a multiple of 8");
+  if (bitorder != SPP_BITORDER_BIG && bitorder != SPP_BITORDER_LITTLE) return fail(SPP_ERR_ARG, "bad bitorder");
+  return SPP_OK;
+}
+
+}  // namespace spp
+
+using namespace spp;
+
+extern "C" {
+
+int spp_bandpass(const void* in, int nbits, int bitorder, int64_t nchans, int64_t nsamps,
+                 float* bpass, void* stream) {
+  int rc = check_raw(in, nbits, bitorder, nchans, nsamps);
+  if (rc) return rc;
+  if (!bpass) return fail(SPP_ERR_ARG, "null bpass");
+  if (nsamps == 0) return SPP_OK;
+  cudaStream_t st = as_stream(stream);
+  const unsigned blocks = (unsigned)ceil_div(nchans, 128);
+  rc = dispatch_nb(nbits, [&](auto nb) {
+    k_bandpass<decltype(nb)::value><<<blocks, 128, 0, st>>>(in, nchans, nsamps, bitorder, bpass);
+  });
+  if (rc) return rc;
+  return cuda_status(cudaGetLastError(), "bandpass launch");
+}
+
+int spp_collapse(const void* in, int nbits, int bitorder, int64_t nchans, int64_t nsamps,
+                 float* tim, int64_t out_start, void* stream) {
+  int rc = check_raw(in, nbits, bitorder, nchans, nsamps);
+  if (rc) return rc;
+  if (!tim || out_start < 0) return fail(SPP_ERR_ARG, "bad output");
+  if (nsamps == 0) return SPP_OK;
+  cudaStream_t st = as_stream(stream);
+  const unsigned blocks = (unsigned)ceil_div(nsamps, 8);
+  rc = dispatch_nb(nbits, [&](auto nb) {
+    k_collapse<decltype(nb)::value><<<blocks, 256, 0, st>>>(in, nchans, nsamps, bitorder, tim, out_start);
+  });
+  if (rc) return rc;
+  return cuda_status(cudaGetLastError(), "collapse launch");
+}
+
+int spp_zero_dm(const float* in, float* out, int64_t nchans, int64_t nsamps, const float* bpass,
+                const float* chanwts, void* stream) {
+  if (!in || !out || !bpass || !chanwts) return fail(SPP_ERR_ARG, "null pointer");
+  if (nchans <= 0 || nsamps < 0) return fail(SPP_ERR_ARG, "bad shape");
+  if (nsamps == 0) return SPP_OK;
+  const unsigned blocks = (unsigned)std::min<int64_t>(nsamps, 148 * 16);
+  k_zero_dm<<<blocks, 256, 0, as_stream(stream)>>>(in, out, nchans, nsamps, bpass, chanwts);
+  return cuda_status(cudaGetLastError(), "zero_dm launch");
+}
+
+int spp_downsample_mean(const float* in, int64_t nrows, int64_t n, int64_t in_stride, int factor,
+                        float* out, int64_t out_stride, void* stream) {
+  if (!in || !out) return fail(SPP_ERR_ARG, "null pointer");
+  if (factor <= 0) return fail(SPP_ERR_ARG, "Factor must be a positive integer.");
+  if (nrows <= 0 || n < 0) return fail(SPP_ERR_ARG, "bad shape");
+  if (factor > n) return fail(SPP_ERR_ARG, "Factor must be less than the size of the array.");
+  if (nrows > 65535) return fail(SPP_ERR_UNSUPPORTED, "too many rows");
+  const int64_t m = n / factor;
+  dim3 grid((unsigned)std::min<int64_t>(ceil_div(m, 256), 4096), (unsigned)nrows);
+  k_downsample<<<grid, 256, 0, as_stream(stream)>>>(in, n, in_stride, factor, out, out_stride);
+  return cuda_status(cudaGetLastError(), "downsample launch");
+}
+
+int spp_downsample_2d_mean(const float* in, int64_t dim1, int64_t dim2, int factor1, int factor2,
+                           float* out, void* stream) {
+  if (!in || !out) return fail(SPP_ERR_ARG, "null pointer");
+  if (factor1 <= 0 || factor2 <= 0) return fail(SPP_ERR_ARG, "factors must be positive");
+  const int64_t total = (dim1 / factor1) * (dim2 / factor2);
+  if (total == 0) return SPP_OK;
+  const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(total, 256), 148 * 32);
+  k_downsample_2d<<<blocks, 256, 0, as_stream(stream)>>>(in, dim1, dim2, factor1, factor2, out);
+  return cuda_status(cudaGetLastError(), "downsample_2d launch");
+}
+
+int spp_subband(const void* in, int nbits, int bitorder, int64_t nchans, int64_t nsamps,
+                const int32_t* delays, int32_t maxdelay, const int32_t* chan_to_sub, int64_t nsub,
+                float* out, void* stream) {
+  int rc = check_raw(in, nbits, bitorder, nchans, nsamps);
+  if (rc) return rc;
+  if (!delays || !chan_to_sub || !out || nsub <= 0) return fail(SPP_ERR_ARG, "bad arguments");
+  const int64_t nout = nsamps - maxdelay;
+  if (nout <= 0) return SPP_OK;
+  cudaStream_t st = as_stream(stream);
+  rc = cuda_status(cudaMemsetAsync(out, 0, sizeof(float) * nout * nsub, st), "subband memset");
+  if (rc) return rc;
+  const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(nout * nchans, 256), 148 * 64);
+  rc = dispatch_nb(nbits, [&](auto nb) {
+    k_subband<decltype(nb)::value><<<blocks, 256, 0, st>>>(in, nchans, nsamps, bitorder, delays,
+                                                           chan_to_sub, nsub, nout, out);
+  });
+  if (rc) return rc;
+  return cuda_status(cudaGetLastError(), "subband launch");
+}
+
+}  // extern "C"
+
+// Sizes the S/N workspace for `n` samples per row.
+int64_t snr_ws(int64_t nrows, int64_t n, int nfactors, int nwidths, int64_t* nchunks) {
+  const int64_t nck = ceil_div(std::max<int64_t>(n, 1), kSnrChunk);
+  *nchunks = nck;
+  const int64_t parts = nrows * nfactors * nwidths * nck * (int64_t)sizeof(SnrPart);
+  const int64_t stats = nrows * nfactors * nck * 3 * (int64_t)sizeof(double);
+  return kStatusBytes + round_up(parts, 256) + round_up(stats, 256);
+}
+
+extern "C" {
+
+int64_t spp_boxcar_snr_workspace_bytes(int64_t nrows, int64_t n, int nfactors, int nwidths) {
+  int64_t nck;
+  return snr_ws(nrows, n, nfactors, nwidths, &nck);
+}
+
+int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n, int64_t in_stride,
+                   const int32_t* factors, int nfactors, const int32_t* widths, int nwidths,
+                   float* snr, int32_t* peak_index, void* workspace, int64_t workspace_bytes,
+                   void* stream) {
+  if (!in || !factors || !widths || !snr || !workspace) return fail(SPP_ERR_ARG, "null pointer");
+  if (in_kind != SPP_OUT_F32 && in_kind != SPP_OUT_I32) return fail(SPP_ERR_ARG, "bad in_kind");
+  if (nrows <= 0 || n <= 0 || nfactors <= 0 || nfactors > 8 || nwidths <= 0 ||
+      nwidths > kSnrMaxWidths)
+    return fail(SPP_ERR_ARG, "bad sizes (nfactors <= 8, nwidths <= %d)", kSnrMaxWidths);
+  if (nrows * nfactors > 65535) return fail(SPP_ERR_UNSUPPORTED, "rows*factors > 65535");
+  SnrCfg cfg{};
+  cfg.nf = nfactors;
+  cfg.nw = nwidths;
+  cfg.wmax = 1;
+  for (int i = 0; i < nfactors; ++i) {
+    if (factors[i] <= 0 || factors[i] > n) return fail(SPP_ERR_ARG, "invalid downsample factor %d", factors[i]);
+    cfg.f[i] = factors[i];
+  }
+  for (int i = 0; i < nwidths; ++i) {
+    if (widths[i] < 1 || widths[i] > kSnrMaxW) return fail(SPP_ERR_ARG, "invalid boxcar width: %d", widths[i]);
+    cfg.w[i] = widths[i];
+    cfg.wmax = std::max(cfg.wmax, (int)widths[i]);
+  }
+  int64_t nck;
+  const int64_t need = snr_ws(nrows, n, nfactors, nwidths, &nck);
+  if (workspace_bytes < need)
+    return fail(SPP_ERR_SIZE, "workspace %lld < %lld", (long long)workspace_bytes, (long long)need);
+  cudaStream_t st = as_stream(stream);
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  SnrPart* parts = reinterpret_cast<SnrPart*>(ws + kStatusBytes);
+  double* stats = reinterpret_cast<double*>(
+      ws + kStatusBytes + round_up(nrows * nfactors * nwidths * nck * (int64_t)sizeof(SnrPart), 256));
+  int rc = cuda_status(cudaMemsetAsync(parts, 0xFF, sizeof(SnrPart) * nrows * nfactors * nwidths * nck, st), "parts init");
+  if (rc) return rc;
+  rc = cuda_status(cudaMemsetAsync(stats, 0, sizeof(double) * 3 * nrows * nfactors * nck, st), "stats init");
+  if (rc) return rc;
+  const int64_t smem = (int64_t)(kSnrChunk + cfg.wmax + 1) * 8;
+  if (smem > 48 * 1024) {
+    rc = cuda_status(cudaFuncSetAttribute(k_snr_chunk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "snr smem");
+    if (rc) return rc;
+  }
+  dim3 grid((unsigned)nck, (unsigned)(nrows * nfactors));
+  k_snr_chunk<<<grid, kSnrThreads, smem, st>>>(in, in_kind, n, in_stride, cfg, nck, parts, stats);
+  rc = cuda_status(cudaGetLastError(), "snr chunk launch");
+  if (rc) return rc;
+  const int64_t nout = nrows * nfactors * nwidths;
+  k_snr_final<<<(unsigned)ceil_div(nout, 256), 256, 0, st>>>(n, cfg, nrows, nck, parts, stats, snr, peak_index);
+  return cuda_status(cudaGetLastError(), "snr final launch");
+}
+
+}  // extern "C"

@@ -1,0 +1,329 @@
+"""Filterbank sources and the streaming drop-in path (R1, R5).
+
+``Filterbank`` carries the reference's streaming operations
+(src/sigpyproc/base.py) over a block schedule identical to
+``FilReader.read_plan`` (src/sigpyproc/readers.py:171-233).  Blocks travel
+as raw bytes: file -> pinned host buffer -> async H2D (copy stream) -> HBM,
+double-buffered, and the GPU kernels unpack them in their load path.  The
+``skipback`` halo is re-read exactly as the reference does, so results are
+identical block for block.
+"""
+
+from __future__ import annotations
+
+from collections.abc import Callable, Iterator
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _lib
+from .block import FilterbankBlock
+from .dedisp import DMTPlan, dedisperse_block, stream_handle, workspace
+from .header import Header
+from .io.bits import bitorder_code
+from .io.bits import unpack as gpu_unpack
+from .timeseries import TimeSeries
+
+
+def plan_blocks(nsamples: int, gulp: int, start: int, nsamps: int | None,
+                skipback: int) -> tuple[int, list[tuple[int, int, int]]]:
+    """Block schedule of read_plan: (gulp, [(ii, samples, skip)])."""
+    if nsamps is None:
+        nsamps = nsamples - start
+    gulp = min(nsamps, gulp)
+    skipback = abs(skipback)
+    if skipback >= gulp:
+        raise ValueError(f"readsamps ({gulp}) must be > skipback ({skipback})")
+    nreads, lastread = divmod(nsamps, (gulp - skipback))
+    if lastread < skipback:
+        nreads -= 1
+        lastread = nsamps - (nreads * (gulp - skipback))
+    blocks = [(ii, gulp, -skipback) for ii in range(nreads)]
+    if lastread != 0:
+        blocks.append((nreads, lastread, 0))
+    return gulp, blocks
+
+
+def pinned_allocator(nbytes: int) -> torch.Tensor:
+    return torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+
+
+def _host_view(buf) -> np.ndarray:
+    if torch.is_tensor(buf):
+        return buf.numpy()
+    return np.frombuffer(memoryview(buf), dtype=np.uint8)
+
+
+def _allocate(allocator: Callable[[int], object], nbytes: int):
+    """io/fileio.py:25-71 contract: positive size, buffer object of that size."""
+    if nbytes <= 0:
+        raise ValueError(f"Requested buffer size ({nbytes}) is invalid, should be > 0")
+    try:
+        buf = allocator(nbytes)
+    except Exception as exc:
+        raise RuntimeError(f"Failed to allocate buffer of size {nbytes}") from exc
+    view = _host_view(buf)
+    if view.nbytes != nbytes:
+        raise ValueError(f"Allocated buffer is not the expected size: {view.nbytes} (actual) "
+                         f"!= {nbytes} (expected)")
+    return buf
+
+
+class Filterbank:
+    """Base of filterbank sources.  Subclasses provide ``header`` and
+    ``_read_bytes(offset, view)`` (fill ``view`` from byte ``offset`` of the
+    data stream, return the byte count)."""
+
+    header: Header
+
+    # --- geometry ---
+    @property
+    def row_bytes(self) -> int:
+        h = self.header
+        return h.nchans * 4 if h.nbits == 32 else h.nchans * h.nbits // 8
+
+    @property
+    def bitorder(self) -> str:
+        return {1: "little", 2: "big", 4: "big"}.get(self.header.nbits, "big")
+
+    def _read_bytes(self, offset: int, view: np.ndarray) -> int:  # pragma: no cover
+        raise NotImplementedError
+
+    # --- streaming (R5) ---
+    def stream_blocks(self, gulp: int = 16384, start: int = 0, nsamps: int | None = None,
+                      skipback: int = 0, *, allocator: Callable[[int], object] | None = None,
+                      description: str | None = None, quiet: bool = False
+                      ) -> Iterator[tuple[int, int, torch.Tensor]]:
+        """Yields ``(nsamps_read, ii, raw)``: ``raw`` is a CUDA uint8 tensor of
+        the block's raw bytes, valid until the next iteration.  Work the
+        consumer enqueues on the current stream is ordered before the buffer
+        is refilled."""
+        gulp, blocks = plan_blocks(self.header.nsamples, gulp, start, nsamps, skipback)
+        rb = self.row_bytes
+        if self.header.nbits < 8 and (self.header.nchans * self.header.nbits) % 8:
+            raise ValueError("nchans * nbits must be a multiple of 8")
+        nbytes = gulp * rb
+        alloc = pinned_allocator if allocator is None else allocator
+        dev = torch.device("cuda", torch.cuda.current_device())
+        host = [_allocate(alloc, nbytes) for _ in range(2)]
+        hviews = [_host_view(h) for h in host]
+        devbuf = [torch.empty(nbytes, dtype=torch.uint8, device=dev) for _ in range(2)]
+        copy_stream = torch.cuda.Stream(dev)
+        compute = torch.cuda.current_stream(dev)
+        copied = [torch.cuda.Event() for _ in range(2)]
+        consumed = [torch.cuda.Event() for _ in range(2)]
+        used = [False, False]
+        pos = start * rb
+        for ii, nsamp_blk, skip in blocks:
+            k = ii & 1
+            want = nsamp_blk * rb
+            if used[k]:
+                copied[k].synchronize()  # host buffer k is free once its copy landed
+            got = self._read_bytes(pos, hviews[k][:want])
+            if got != want:
+                raise ValueError(f"Unexpected number of bytes read from file {got} (actual) "
+                                 f"!= {want} (expected)")
+            pos += want + skip * rb
+            with torch.cuda.stream(copy_stream):
+                if used[k]:
+                    copy_stream.wait_event(consumed[k])
+                src = host[k] if torch.is_tensor(host[k]) else torch.from_numpy(hviews[k])
+                devbuf[k][:want].copy_(src[:want], non_blocking=True)
+                copied[k].record(copy_stream)
+            compute.wait_event(copied[k])
+            used[k] = True
+            yield nsamp_blk, ii, devbuf[k][:want]
+            consumed[k].record(compute)
+        torch.cuda.current_stream(dev).synchronize()
+
+    def read_plan(self, gulp: int = 16384, start: int = 0, nsamps: int | None = None,
+                  skipback: int = 0, description: str | None = None, *, quiet: bool = False,
+                  allocator: Callable[[int], object] | None = None
+                  ) -> Iterator[tuple[int, int, np.ndarray]]:
+        """Reference-compatible read_plan: yields host arrays of the block's
+        samples (unpacked to one uint8 per sample for nbits < 8, on the GPU)."""
+        h = self.header
+        for nsamp_blk, ii, raw in self.stream_blocks(gulp, start, nsamps, skipback,
+                                                     allocator=allocator):
+            if h.nbits in (1, 2, 4):
+                data = gpu_unpack(raw, h.nbits, self.bitorder).cpu().numpy()
+            elif h.nbits == 32:
+                data = raw.view(torch.float32).cpu().numpy()
+            else:
+                data = raw.cpu().numpy()
+            yield nsamp_blk, ii, data
+
+    # --- R1: single-DM dedispersion ---
+    def dedisperse(self, dm: float, ref_freq: str | float = "fch1", gulp: int = 16384,
+                   start: int = 0, nsamps: int | None = None, *, parallel: bool = False,
+                   **plan_kwargs) -> TimeSeries:
+        """Dedisperse and collapse to a time series (base.py:360-424).
+
+        ``parallel`` is accepted for compatibility; the GPU path is always
+        parallel.  Float32 data is accumulated in float64 like the reference.
+        """
+        del parallel
+        h = self.header
+        chan_delays = np.atleast_1d(h.get_dmdelays(dm, ref_freq)).astype(np.int32)
+        max_delay = int(np.max(np.abs(chan_delays)))
+        gulp = max(2 * max_delay, gulp)
+        tim_len = h.nsamples - max_delay
+        dev = torch.device("cuda", torch.cuda.current_device())
+        tim = torch.zeros(max(tim_len, 0), dtype=torch.float32, device=dev)
+        ddev = torch.from_numpy(chan_delays).to(dev)
+        for nsamps_r, ii, raw in self.stream_blocks(gulp, start, nsamps, skipback=max_delay,
+                                                    **plan_kwargs):
+            dedisperse_block(raw, chan_delays, h.nchans, nsamps_r, tim, ii * (gulp - max_delay),
+                             nbits=h.nbits, bitorder=self.bitorder, acc=_lib.ACC_F64,
+                             delays_dev=ddev)
+        return TimeSeries(tim, h.new_header({"nchans": 1, "dm": dm, "nsamples": tim_len}))
+
+    # --- R3: DM-trial batch ---
+    def dedisperse_batch(self, dms=None, *, dm: float | None = None, dmsteps: int = 512,
+                         ref_freq: str | float = "fch1", gulp: int = 1 << 20, start: int = 0,
+                         nsamps: int | None = None, out_dtype=None, **plan_kwargs):
+        """DM-time array ``out[i][t] = dedisperse(dms[i])[t]`` over the valid
+        samples common to every trial (``nsamples - max_i max_c |delay|``).
+
+        Give ``dms`` explicitly or ``dm``/``dmsteps`` for the dmt_transform
+        grid ``dm + linspace(-dm, dm, dmsteps)``.  Integer data defaults to
+        exact int32 sums, float data to float32.  Returns (tensor, dms).
+        """
+        h = self.header
+        if dms is None:
+            if dm is None:
+                raise ValueError("give dms or dm/dmsteps")
+            dms = dm + np.linspace(-dm, dm, dmsteps)
+        dms = np.atleast_1d(np.asarray(dms, dtype=np.float64))
+        delays = np.atleast_2d(h.get_dmdelays(dms, ref_freq)).astype(np.int32)
+        max_delay = int(np.max(np.abs(delays)))
+        if out_dtype is None:
+            out_dtype = torch.float32 if h.nbits == 32 else torch.int32
+        gulp = max(2 * max_delay, gulp)
+        span = (h.nsamples - start) if nsamps is None else nsamps
+        nout = max(span - max_delay, 0)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        out = torch.zeros((delays.shape[0], nout), dtype=out_dtype, device=dev)
+        plan = DMTPlan(delays, h.nchans, min(gulp, span), nbits=h.nbits, bitorder=self.bitorder,
+                       out_dtype=out_dtype)
+        try:
+            for nsamps_r, ii, raw in self.stream_blocks(gulp, start, nsamps, skipback=max_delay,
+                                                        **plan_kwargs):
+                plan.execute(raw, nsamps_r, out, out_start=ii * (gulp - max_delay))
+        finally:
+            torch.cuda.current_stream(dev).synchronize()
+            plan.close()
+        return out, dms
+
+    # --- channel statistics (R10 / N2) ---
+    def bandpass(self, method: str = "sum", gulp: int = 16384, start: int = 0, *,
+                 parallel: bool = False, nsamps: int | None = None, **plan_kwargs) -> TimeSeries:
+        """Per-channel sum (or mean) over samples (base.py:308-358), float32
+        accumulated in sample order exactly as the reference."""
+        del parallel
+        h = self.header
+        dev = torch.device("cuda", torch.cuda.current_device())
+        bp = torch.zeros(h.nchans, dtype=torch.float32, device=dev)
+        total = 0
+        for nsamps_r, _ii, raw in self.stream_blocks(gulp, start, nsamps, **plan_kwargs):
+            _lib.call("spp_bandpass", raw.data_ptr(), h.nbits, bitorder_code(self.bitorder),
+                      h.nchans, nsamps_r, bp.data_ptr(), stream_handle(None, dev))
+            total += nsamps_r
+        if method == "mean":
+            bp /= total
+        return TimeSeries(bp, h.new_header({"nchans": 1, "nsamples": h.nchans}))
+
+    def collapse(self, method: str = "sum", gulp: int = 16384, start: int = 0,
+                 nsamps: int | None = None, *, parallel: bool = False,
+                 **plan_kwargs) -> TimeSeries:
+        """Sum over channels per sample (base.py:256-306)."""
+        del parallel
+        h = self.header
+        tim_len = (h.nsamples - start) if nsamps is None else nsamps
+        dev = torch.device("cuda", torch.cuda.current_device())
+        tim = torch.zeros(tim_len, dtype=torch.float32, device=dev)
+        for nsamps_r, ii, raw in self.stream_blocks(gulp, start, nsamps, **plan_kwargs):
+            # the reference offsets each block by ii * nsamps_r (base.py:292-298)
+            _lib.call("spp_collapse", raw.data_ptr(), h.nbits, bitorder_code(self.bitorder),
+                      h.nchans, nsamps_r, tim.data_ptr(), ii * nsamps_r, stream_handle(None, dev))
+        if method == "mean":
+            tim /= h.nchans
+        return TimeSeries(tim, h.new_header({"nchans": 1, "dm": 0}))
+
+
+class FilReader(Filterbank):
+    """Sigproc filterbank file(s) (readers.py:33-233)."""
+
+    def __init__(self, filenames, *, check_contiguity: bool = True):
+        if isinstance(filenames, (str, Path)):
+            filenames = [filenames]
+        self._filenames = [str(f) for f in filenames]
+        self._header = Header.from_sigproc(self._filenames)
+        del check_contiguity
+
+    @property
+    def header(self) -> Header:
+        return self._header
+
+    @property
+    def filename(self) -> str:
+        return self._filenames[0]
+
+    def _read_bytes(self, offset: int, view: np.ndarray) -> int:
+        info = self._header.stream
+        done = 0
+        want = view.nbytes
+        base = 0
+        for fname, hlen, dlen in zip(info.files, info.hdrlens, info.datalens):
+            if offset + done < base + dlen and done < want:
+                local = offset + done - base
+                n = min(dlen - local, want - done)
+                with open(fname, "rb") as fp:
+                    fp.seek(hlen + local)
+                    got = fp.readinto(memoryview(view[done:done + n]))
+                done += got or 0
+            base += dlen
+        return done
+
+    def read_block(self, start: int, nsamps: int, fch1: float | None = None,
+                   nchans: int | None = None) -> FilterbankBlock:
+        """(nchans, nsamps) float32 block in HBM (readers.py:98-130)."""
+        h = self.header
+        fch1 = h.fch1 if fch1 is None else fch1
+        nchans = h.nchans if nchans is None else nchans
+        if fch1 > h.fch1 or nchans > h.nchans:
+            raise ValueError(f"requested block is out of range: fch1={fch1}, nchans={nchans}")
+        if start < 0 or start + nsamps > h.nsamples:
+            raise ValueError(f"requested block is out of range: start={start}, nsamps={nsamps}")
+        raw = np.empty(nsamps * self.row_bytes, dtype=np.uint8)
+        got = self._read_bytes(start * self.row_bytes, raw)
+        raw_t = torch.from_numpy(raw[:got]).cuda()
+        if h.nbits in (1, 2, 4):
+            vals = gpu_unpack(raw_t, h.nbits, self.bitorder).view(-1, h.nchans).float()
+        elif h.nbits == 32:
+            vals = raw_t.view(torch.float32).view(-1, h.nchans)
+        else:
+            vals = raw_t.view(-1, h.nchans).float()
+        chan_start = int((fch1 - h.fch1) / h.foff)
+        data = vals.t()[chan_start:chan_start + nchans].contiguous()
+        hdr = h.new_header({"tstart": h.mjd_after_nsamps(start), "nsamples": data.shape[1],
+                            "fch1": fch1, "nchans": nchans})
+        return FilterbankBlock(data, hdr)
+
+
+class ArrayFilterbank(Filterbank):
+    """A filterbank held in host memory (raw time-major bytes), e.g. synthetic data."""
+
+    def __init__(self, raw: np.ndarray, header: Header):
+        self._raw = np.ascontiguousarray(raw).view(np.uint8).ravel()
+        self._header = header
+
+    @property
+    def header(self) -> Header:
+        return self._header
+
+    def _read_bytes(self, offset: int, view: np.ndarray) -> int:
+        n = max(0, min(view.nbytes, self._raw.nbytes - offset))
+        view[:n] = self._raw[offset:offset + n]
+        return n

@@ -1,0 +1,267 @@
+"""Generate golden vectors by running the REFERENCE implementation's own code.
+
+Run in a container where the reference source tree is mounted (path from
+$SPP_REFERENCE_ROOT, default /root/reference):
+
+    python tests/golden/make_golden.py
+
+It loads src/sigpyproc/core/kernels.py (numba) and single functions of
+params.py / header.py / readers.py through oracle/refload.py, evaluates them
+on seeded inputs and writes the outputs next to this script.  The GPU tests
+and the oracle tests compare against these files; nothing at test time reads
+the reference tree.
+"""
+
+from __future__ import annotations
+
+import hashlib
+import json
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+
+from oracle import refload  # noqa: E402
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main() -> None:
+    if not refload.available():
+        raise SystemExit("reference tree not found")
+    K = refload.load_kernels()
+    cdd, dmc = refload.load_compute_dmdelays()
+    hf = refload.load_header_freq_helpers()
+    read_plan = refload.load_read_plan()
+
+    class Hdr:
+        def __init__(self, nchans, fch1, foff):
+            self.nchans, self.fch1, self.foff = nchans, fch1, foff
+
+        @property
+        def chan_freqs(self):
+            return hf["chan_freqs"](self)
+
+        @property
+        def ftop(self):
+            return hf["ftop"](self)
+
+        @property
+        def fcenter(self):
+            return hf["fcenter"](self)
+
+        @property
+        def fbottom(self):
+            return hf["fbottom"](self)
+
+        @property
+        def fmax(self):
+            return hf["fmax"](self)
+
+        @property
+        def fmin(self):
+            return hf["fmin"](self)
+
+    def ref_delays(nchans, fch1, foff, tsamp, dm, ref="fch1"):
+        h = Hdr(nchans, fch1, foff)
+        fref = float(getattr(h, ref)) if isinstance(ref, str) else float(ref)
+        return cdd(h.chan_freqs, dm, tsamp, fref)
+
+    out: dict[str, np.ndarray] = {}
+    meta: dict = {"dm_constant": dmc}
+
+    # ---- R4 unpack: the reference KAT input [7, 23] and a random byte array
+    rng = np.random.default_rng(11)
+    rnd = rng.integers(0, 256, size=4096, dtype=np.uint8)
+    out["unpack_rand_in"] = rnd
+    for nbits in (1, 2, 4):
+        for order in ("big", "little"):
+            fn = getattr(K, f"unpack{nbits}_8_{order}")
+            for tag, arr in (("kat", np.array([7, 23], dtype=np.uint8)), ("rand", rnd)):
+                u = np.empty(arr.size * 8 // nbits, dtype=np.uint8)
+                fn(arr, u)
+                out[f"unpack_{tag}_{nbits}_{order}"] = u
+
+    # ---- R6 delays at the benchmark geometries and the reference test geometry
+    geoms = {
+        "c1": (256, 1500.0, -1.0, 64e-6, np.array([100.0])),
+        "c2": (4096, 1500.0, -0.0732421875, 64e-6, 1000.0 + np.linspace(-1000.0, 1000.0, 1024)),
+        "c3": (1024, 1400.0, -0.29296875, 64e-6, 500.0 + np.linspace(-500.0, 500.0, 512)),
+        "c5": (4096, 1500.0, -0.0732421875, 64e-6, 1500.0 + np.linspace(-1500.0, 1500.0, 4096)),
+        "parkes": (832, 4030.0, -4.0, 512e-6, np.array([0.0, 100.0, 5000.0])),
+        "tutorial": (64, 1510.0, -1.09, 320e-6, np.array([10.0, 50.0, 200.0])),
+    }
+    meta["delays"] = {}
+    for name, (nch, f1, fo, ts, dms) in geoms.items():
+        for ref in ("fch1", "fcenter", "fmax", "fmin", 1234.5):
+            if name in ("c2", "c5") and ref != "fch1":
+                continue
+            d = np.atleast_2d(ref_delays(nch, f1, fo, ts, dms, ref)).astype(np.int32)
+            key = f"{name}_{ref}"
+            meta["delays"][key] = {
+                "geom": [nch, f1, fo, ts], "ref": ref, "ndm": int(d.shape[0]),
+                "sha256": sha(d), "max": int(d.max()), "min": int(d.min()),
+            }
+            rows = sorted({0, min(1, d.shape[0] - 1), d.shape[0] // 2, d.shape[0] - 1})
+            out[f"delays_{key}_rows"] = d[rows]
+            out[f"delays_{key}_rowidx"] = np.array(rows, dtype=np.int64)
+            out[f"delays_{key}_dms"] = np.asarray(dms, dtype=np.float64)
+    # float (seconds) delays as the reference test geometry uses
+    freqs = np.arange(1000, dtype=np.float32) * (-1.0) + 1400
+    out["delays_params_sec"] = cdd(freqs, np.linspace(0, 100, 50), 0.001, freqs[0], in_samples=False)
+    out["delays_params_samp"] = cdd(freqs, np.linspace(0, 100, 50), 0.001, freqs[0])
+
+    # ---- R2 dedisperse on seeded small blocks
+    rng = np.random.default_rng(12)
+    u8 = rng.integers(0, 256, size=(4096, 64), dtype=np.uint8)
+    out["ded_u8_in"] = u8
+    for tag, dm, ref in (("dm50", 50.0, "fch1"), ("dm200", 200.0, "fch1"),
+                         ("dm120_fcenter", 120.0, "fcenter")):
+        d = ref_delays(64, 1510.0, -1.09, 320e-6, dm, ref).astype(np.int32)
+        maxd = int(np.max(np.abs(d)))
+        o = np.zeros(4096 - maxd, dtype=np.float32)
+        K.dedisperse(u8.ravel(), o, d, 64, 4096, 0)
+        out[f"ded_u8_{tag}_delays"] = d
+        out[f"ded_u8_{tag}_out"] = o
+    rng = np.random.default_rng(13)
+    f32 = rng.normal(0.0, 1.0, size=(2048, 32)).astype(np.float32)
+    out["ded_f32_in"] = f32
+    d = ref_delays(32, 1400.0, -2.0, 256e-6, 30.0).astype(np.int32)
+    o = np.zeros(2048 - int(np.max(np.abs(d))), dtype=np.float32)
+    K.dedisperse(f32.ravel(), o, d, 32, 2048, 0)
+    out["ded_f32_delays"] = d
+    out["ded_f32_out"] = o
+
+    # ---- R1 at config 1: the full Filterbank.dedisperse flow (read_plan blocks)
+    from sigpyproc3_b200 import synth  # noqa: PLC0415
+
+    c1 = synth.c1_filterbank(1)
+    meta["c1_input_sha256"] = sha(c1)
+    d = ref_delays(256, 1500.0, -1.0, 64e-6, 100.0).astype(np.int32)
+    maxd = int(np.max(np.abs(d)))
+    gulp = max(2 * maxd, 16384)
+    tim = np.zeros(65536 - maxd, dtype=np.float32)
+
+    class FakeFile:
+        def __init__(self, raw):
+            self.raw = raw
+            self.pos = 0
+            self.reads = []
+
+        def seek(self, offset, whence=0):
+            self.pos = offset if whence == 0 else self.pos + offset
+
+        def creadinto(self, rbuf, ubuf=None):
+            mv = memoryview(rbuf)
+            n = min(len(mv), self.raw.size - self.pos)
+            np.frombuffer(mv, dtype=np.uint8)[:n] = self.raw[self.pos:self.pos + n]
+            self.reads.append(self.pos)
+            self.pos += n
+            return n
+
+    class FakeReader:
+        def __init__(self, raw, nsamples, nchans, itemsize=1):
+            self.header = type("H", (), {"nsamples": nsamples, "nchans": nchans})()
+            self.bitsinfo = type("B", (), {"unpack": False, "dtype": np.dtype(np.uint8)})()
+            self.samp_stride = nchans * itemsize
+            self.chan_stride = float(itemsize)
+            self._file = FakeFile(raw)
+
+    fr = FakeReader(c1, 65536, 256)
+    for nsamps_r, ii, data in read_plan(fr, gulp=gulp, skipback=maxd, quiet=True):
+        K.dedisperse(np.ascontiguousarray(data), tim, d, 256, nsamps_r, ii * (gulp - maxd))
+    out["c1_tim"] = tim
+    out["c1_delays"] = d
+
+    # ---- R5 read_plan schedules (byte offsets of each read and the yielded sizes)
+    plans = []
+    for nsamples, nchans, gulp, start, nsamps, skip in (
+        (4096, 832, 512, 0, None, 0), (4096, 832, 400, 0, None, 200), (4096, 832, 512, 0, 1024, 0),
+        (65536, 256, 16384, 0, None, 1301), (10000, 64, 3000, 17, 5000, 999),
+        (10000, 64, 2000, 0, None, 500), (3000, 64, 1000, 0, None, 900),
+        (1000, 16, 5000, 0, None, 10),
+    ):
+        raw = (np.arange(nsamples * nchans) % 251).astype(np.uint8)
+        fr = FakeReader(raw, nsamples, nchans)
+        rec = []
+        error = None
+        try:
+            for nsamps_r, ii, data in read_plan(fr, gulp=gulp, start=start, nsamps=nsamps,
+                                                skipback=skip, quiet=True):
+                rec.append([int(nsamps_r), int(ii), int(fr._file.reads[-1]),
+                            sha(np.asarray(data))])
+        except ValueError as exc:
+            # the reference reads a full gulp for a short last block when the
+            # file continues past start+nsamps, and then rejects the byte count
+            error = str(exc)
+        plans.append({"args": [nsamples, nchans, gulp, start, nsamps, skip], "blocks": rec,
+                      "error": error})
+    errs = []
+    for nsamples, gulp, nsamps, skip in ((4096, 512, 1024, 1024), (4096, 512, 1024, 2000)):
+        fr = FakeReader(np.zeros(nsamples * 8, np.uint8), nsamples, 8)
+        try:
+            list(read_plan(fr, gulp=gulp, nsamps=nsamps, skipback=skip, quiet=True))
+            errs.append({"args": [nsamples, gulp, nsamps, skip], "error": None})
+        except ValueError as exc:
+            errs.append({"args": [nsamples, gulp, nsamps, skip], "error": str(exc)})
+    meta["read_plan"] = plans
+    meta["read_plan_errors"] = errs
+
+    # ---- R3 compat: kernels.dmt_block on a float block (nchans, nsamps)
+    rng = np.random.default_rng(14)
+    blk = rng.normal(0, 1, size=(32, 512)).astype(np.float32)
+    dmd = np.atleast_2d(ref_delays(32, 1400.0, -2.0, 256e-6, 10.0 + np.linspace(-10, 10, 16)))
+    out["dmt_block_in"] = blk
+    out["dmt_block_delays"] = dmd.astype(np.int64)
+    out["dmt_block_out"] = K.dmt_block(blk, dmd.astype(np.int64))
+    # integer-valued block (exact in float32)
+    blk_i = rng.integers(0, 4, size=(32, 512)).astype(np.float32)
+    out["dmt_block_int_in"] = blk_i
+    out["dmt_block_int_out"] = K.dmt_block(blk_i, dmd.astype(np.int64))
+
+    # ---- R7 kernels.subband (zero-initialised output)
+    rng = np.random.default_rng(15)
+    sb_in = rng.integers(0, 256, size=(2048, 64), dtype=np.uint8)
+    d = ref_delays(64, 1510.0, -1.09, 320e-6, 80.0).astype(np.int32)
+    maxd = int(np.max(np.abs(d)))
+    c2s = (np.arange(64, dtype=np.int32) // 8).astype(np.int32)
+    sb_out = np.zeros((2048 - maxd) * 8, dtype=np.float32)
+    K.subband(sb_in.ravel(), sb_out, d, c2s, np.int32(maxd), np.int32(64), np.int32(8), np.int32(2048))
+    out["subband_in"] = sb_in
+    out["subband_delays"] = d
+    out["subband_out"] = sb_out
+
+    # ---- R10 bandpass / zero-DM / collapse, R8 downsample
+    rng = np.random.default_rng(16)
+    zf = rng.normal(5.0, 2.0, size=(1024, 48)).astype(np.float32)
+    bp = np.zeros(48, dtype=np.float32)
+    K.extract_bpass(zf.ravel(), bp, 48, 1024)
+    zo = np.empty_like(zf.ravel())
+    K.remove_zerodm(zf.ravel(), zo, bp, 48, 1024)
+    out["zdm_in"] = zf
+    out["zdm_bpass"] = bp
+    out["zdm_out"] = zo.reshape(1024, 48)
+    bpu = np.zeros(64, dtype=np.float32)
+    K.extract_bpass(u8.ravel(), bpu, 64, 4096)
+    out["bpass_u8"] = bpu
+    tim = np.zeros(4096, dtype=np.float32)
+    K.extract_tim(u8.ravel(), tim, 64, 4096, 0)
+    out["collapse_u8"] = tim
+    ds_in = rng.normal(0, 1, size=10007).astype(np.float32)
+    out["ds_in"] = ds_in
+    for f in (1, 2, 4, 7):
+        out[f"ds_out_{f}"] = K.downsample_1d_mean(ds_in, f)
+
+    np.savez_compressed(HERE / "golden.npz", **out)
+    (HERE / "golden.json").write_text(json.dumps(meta, indent=1))
+    print(f"wrote {len(out)} arrays, {(HERE / 'golden.npz').stat().st_size} bytes")
+
+
+if __name__ == "__main__":
+    main()

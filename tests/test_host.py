@@ -1,0 +1,154 @@
+"""Host-side logic without a GPU: delay tables (R6) against the reference's own
+outputs, the read_plan schedule (R5), sigproc headers (N1), and the C ABI
+library's exported symbols."""
+
+import ctypes
+import hashlib
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def test_delays_match_reference(golden, golden_meta):
+    from sigpyproc3_b200.header import Header
+
+    for key, m in golden_meta["delays"].items():
+        nch, f1, fo, ts = m["geom"]
+        h = Header(nchans=nch, fch1=f1, foff=fo, tsamp=ts)
+        dms = golden[f"delays_{key}_dms"]
+        d = np.atleast_2d(h.get_dmdelays(dms, m["ref"])).astype(np.int32)
+        assert sha(d) == m["sha256"], key
+        np.testing.assert_array_equal(d[golden[f"delays_{key}_rowidx"]], golden[f"delays_{key}_rows"])
+
+
+def test_delays_float_and_params(golden):
+    from sigpyproc3_b200 import params
+
+    freqs = np.arange(1000, dtype=np.float32) * (-1.0) + 1400
+    sec = params.compute_dmdelays(freqs, np.linspace(0, 100, 50), 0.001, freqs[0], in_samples=False)
+    assert sec.dtype == np.float32
+    np.testing.assert_array_equal(sec, golden["delays_params_sec"])
+    samp = params.compute_dmdelays(freqs, np.linspace(0, 100, 50), 0.001, freqs[0])
+    assert samp.dtype == np.int32
+    np.testing.assert_array_equal(samp, golden["delays_params_samp"])
+    assert np.all(samp[:, 0] == 0)
+
+
+def test_delays_float64_would_differ():
+    # K2: recomputing in float64 changes some delays at the config-2 geometry
+    from sigpyproc3_b200 import synth
+
+    g = synth.C2
+    dms = synth.dm_grid(1000.0, 1024)
+    d32 = g.delays(dms)
+    f = g.chan_freqs().astype(np.float64)
+    d64 = np.rint(dms[:, None] * 4148.808 * (f**-2 - g.fch1**-2) / g.tsamp).astype(np.int32)
+    assert np.count_nonzero(d32 != d64) > 0
+
+
+def test_header_ref_freq_errors():
+    from sigpyproc3_b200.header import Header
+
+    h = Header(nchans=64, fch1=1510.0, foff=-1.09, tsamp=320e-6)
+    with pytest.raises(ValueError):
+        h.get_dmdelays(100, ref_freq="top")
+    with pytest.raises(TypeError):
+        h.get_dmdelays(100, ref_freq=[1.0])
+    assert h.get_dmdelays(0).max() == 0
+
+
+def test_read_plan_schedule(golden_meta):
+    from sigpyproc3_b200.readers import plan_blocks
+
+    for case in golden_meta["read_plan"]:
+        nsamples, nchans, gulp, start, nsamps, skip = case["args"]
+        g, blocks = plan_blocks(nsamples, gulp, start, nsamps, skip)
+        pos = start * nchans
+        ours = []
+        for ii, nblk, sk in blocks:
+            ours.append((nblk, ii, pos))
+            pos += nblk * nchans + sk * nchans
+        ref = [(b[0], b[1], b[2]) for b in case["blocks"]]
+        if case["error"] is None:
+            assert ours == ref
+        else:
+            # the reference stops where its read size check fails; the schedule
+            # up to there is identical
+            assert ours[: len(ref)] == ref
+    for case in golden_meta["read_plan_errors"]:
+        nsamples, gulp, nsamps, skip = case["args"]
+        with pytest.raises(ValueError, match=re.escape(case["error"])):
+            plan_blocks(nsamples, gulp, 0, nsamps, skip)
+
+
+def test_sigproc_roundtrip(tmp_path):
+    from sigpyproc3_b200.header import Header
+    from sigpyproc3_b200.io import sigproc
+
+    h = Header(nchans=64, fch1=1510.0, foff=-1.09, tsamp=320e-6, nbits=2, tstart=59000.5,
+               source="J0000+0000")
+    raw = np.arange(1000 * 16, dtype=np.uint8) % 251
+    p = tmp_path / "x.fil"
+    h.write_sigproc(p, raw)
+    h2 = Header.from_sigproc(p)
+    assert (h2.nchans, h2.nbits, h2.nsamples) == (64, 2, 1000)
+    assert h2.fch1 == 1510.0 and h2.foff == -1.09 and h2.tsamp == 320e-6
+    assert h2.source == "J0000+0000"
+    d = sigproc.read_header(p)
+    assert d["datalen"] == raw.nbytes
+    with pytest.raises(OSError):
+        bad = tmp_path / "bad.fil"
+        bad.write_bytes(b"\x05\x00\x00\x00hello")
+        sigproc.read_header(bad)
+
+
+def test_reference_fixture_headers():
+    # the reference's own sample files parse (only where the tree is mounted)
+    data = Path("/root/reference/tests/data")
+    if not data.is_dir():
+        pytest.skip("reference test data not mounted")
+    from sigpyproc3_b200.header import Header
+
+    h = Header.from_sigproc(data / "parkes_4bit.fil")
+    assert (h.nchans, h.nbits) == (832, 4)
+    assert abs(h.get_dmdelays(100, in_samples=False).max() - 0.8) < 0.1  # test_header.py:35-41
+    assert abs(h.get_dmdelays(5000, in_samples=False).max() - 40.4) < 0.1
+
+
+def _header_functions():
+    text = (ROOT / "include" / "sppgpu.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(spp_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from sigpyproc3_b200 import _lib
+
+    lib = ctypes.CDLL(str(_lib.LIB_PATH))
+    names = _header_functions()
+    assert len(names) > 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python binding covers them with signatures
+    unbound = [n for n in names if n not in _lib.SIGNATURES]
+    assert not unbound, unbound
+
+
+def test_abi_argument_errors_without_gpu():
+    from sigpyproc3_b200 import _lib
+
+    lib = _lib.load()
+    assert lib.spp_unpack(None, 10, 2, 0, None, None) == _lib.SPP_ERR_ARG
+    assert b"null" in lib.spp_last_error_string()
+    assert lib.spp_dedisperse_workspace_bytes(3, 64, 100, 0, 10) == -1
+    assert lib.spp_dedisperse_workspace_bytes(8, 64, 4096, 0, 100) > 64 * 4096
+    # nchans * nbits not a multiple of 8
+    assert lib.spp_dedisperse_workspace_bytes(2, 3, 4096, 0, 10) == -1

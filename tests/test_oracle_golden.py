@@ -1,0 +1,113 @@
+"""The CPU oracle against golden vectors produced by the reference's own code
+(tests/golden/make_golden.py).  This pins the oracle before it checks the GPU."""
+
+import hashlib
+
+import numpy as np
+import pytest
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("nbits", [1, 2, 4])
+@pytest.mark.parametrize("order", ["big", "little"])
+def test_unpack(orc, golden, nbits, order):
+    # reference KAT (tests/test_kernels.py:9-41 input [7, 23]) and a random array
+    kat = orc.unpack(np.array([7, 23], np.uint8), nbits, order)
+    np.testing.assert_array_equal(kat, golden[f"unpack_kat_{nbits}_{order}"])
+    rnd = orc.unpack(golden["unpack_rand_in"], nbits, order)
+    np.testing.assert_array_equal(rnd, golden[f"unpack_rand_{nbits}_{order}"])
+
+
+@pytest.mark.parametrize("tag", ["dm50", "dm200", "dm120_fcenter"])
+def test_dedisperse_u8(orc, golden, tag):
+    x = golden["ded_u8_in"]
+    d = golden[f"ded_u8_{tag}_delays"]
+    out = orc.dedisperse(x.ravel(), d, 64, 4096)
+    np.testing.assert_array_equal(out, golden[f"ded_u8_{tag}_out"])  # bit-exact
+
+
+def test_dedisperse_f32(orc, golden):
+    x = golden["ded_f32_in"]
+    out = orc.dedisperse(x.ravel(), golden["ded_f32_delays"], 32, 2048)
+    # reference uses fastmath (may reassociate the f64 sum): float32 results agree
+    np.testing.assert_allclose(out, golden["ded_f32_out"], rtol=1e-6, atol=1e-6)
+
+
+def test_c1_full(orc, golden, golden_meta):
+    from sigpyproc3_b200 import synth
+
+    raw = synth.c1_filterbank(1)
+    assert sha(raw) == golden_meta["c1_input_sha256"]
+    out = orc.dedisperse(raw, golden["c1_delays"], 256, 65536)
+    np.testing.assert_array_equal(out, golden["c1_tim"])
+
+
+def test_dmt_roll(orc, golden):
+    blk = golden["dmt_block_in"]  # (nchans, nsamps)
+    d = golden["dmt_block_delays"].astype(np.int32)
+    out = orc.dmt_roll(blk.T.copy(), d, 32, 512)
+    np.testing.assert_allclose(out, golden["dmt_block_out"], rtol=1e-5, atol=1e-5)
+    out_i = orc.dmt_roll(golden["dmt_block_int_in"].T.copy(), d, 32, 512)
+    np.testing.assert_array_equal(out_i, golden["dmt_block_int_out"])
+
+
+def test_dmt_rowwise_matches_dedisperse(orc, golden):
+    x = golden["ded_u8_in"]
+    d = np.stack([golden["ded_u8_dm50_delays"], golden["ded_u8_dm200_delays"]])
+    nvalid = 4096 - int(np.abs(d).max())
+    out = orc.dmt(x.ravel(), d, 64, 4096, nvalid)
+    np.testing.assert_array_equal(out[0], golden["ded_u8_dm50_out"][:nvalid])
+    np.testing.assert_array_equal(out[1], golden["ded_u8_dm200_out"][:nvalid])
+
+
+def test_dmt_packed(orc, golden):
+    rnd = golden["unpack_rand_in"]  # 4096 bytes = 2-bit, 64 ch x 256 samples
+    d = np.stack([golden["ded_u8_dm50_delays"] % 50])
+    un = golden["unpack_rand_2_big"]
+    nvalid = 256 - int(d.max())
+    a = orc.dmt_packed(rnd, 2, "big", d, 64, 256, nvalid)
+    b = orc.dmt(un, d, 64, 256, nvalid)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_subband(orc, golden):
+    x = golden["subband_in"]
+    d = golden["subband_delays"]
+    c2s = (np.arange(64) // 8).astype(np.int32)
+    out = orc.subband(x.ravel(), d, c2s, int(np.abs(d).max()), 64, 8, 2048)
+    np.testing.assert_array_equal(out, golden["subband_out"])
+
+
+def test_bandpass_collapse(orc, golden):
+    x = golden["ded_u8_in"]
+    np.testing.assert_array_equal(orc.bandpass(x.ravel(), 64, 4096), golden["bpass_u8"])
+    zf = golden["zdm_in"]
+    np.testing.assert_array_equal(orc.bandpass(zf.ravel(), 48, 1024), golden["zdm_bpass"])
+
+
+def test_zero_dm(orc, golden):
+    out = orc.zero_dm(golden["zdm_in"].ravel(), 48, 1024, golden["zdm_bpass"])
+    np.testing.assert_allclose(out.reshape(1024, 48), golden["zdm_out"], rtol=1e-6, atol=1e-5)
+
+
+@pytest.mark.parametrize("f", [1, 2, 4, 7])
+def test_downsample(orc, golden, f):
+    np.testing.assert_array_equal(orc.downsample_mean(golden["ds_in"], f), golden[f"ds_out_{f}"])
+
+
+def test_boxcar_snr_small(orc):
+    rng = np.random.default_rng(3)
+    x = rng.normal(0, 1, 1000).astype(np.float32)
+    x[500:508] += 3.0
+    snr, idx = orc.boxcar_snr(x, [1, 2], [1, 8])
+    # brute-force check in float64
+    for fi, f in enumerate([1, 2]):
+        y = orc.downsample_mean(x, f).astype(np.float64)
+        mu, sd = y.mean(), y.std()
+        for wi, w in enumerate([1, 8]):
+            s = np.array([y[t:t + w].sum() for t in range(y.size - w + 1)])
+            assert idx[0, fi, wi] == int(np.argmax(s))
+            assert np.isclose(snr[0, fi, wi], (s.max() - w * mu) / (sd * np.sqrt(w)), rtol=1e-12)
