@@ -118,6 +118,13 @@ int spp_dmt_plan_describe(const spp_dmt_plan* plan, int32_t* cfg);
 /* override the tile shape (autotuner); variant index in [0, n) */
 int spp_dmt_plan_num_variants(const spp_dmt_plan* plan);
 int spp_dmt_plan_set_variant(spp_dmt_plan* plan, int variant);
+/* Per-kernel device timing: while enabled, each execute records CUDA events on
+ * its stream around the corner turn and the DM-time kernel;
+ * spp_dmt_plan_timing_read synchronises them and returns the summed
+ * milliseconds and the number of executions since enabling. */
+int spp_dmt_plan_timing(spp_dmt_plan* plan, int enable);
+int spp_dmt_plan_timing_read(spp_dmt_plan* plan, double* ms_corner_turn,
+                             double* ms_dmt, int32_t* nexec);
 int spp_dmt_execute(const spp_dmt_plan* plan, const void* in, int64_t nsamps,
                     void* out, int64_t out_stride, int64_t out_start,
                     void* workspace, int64_t workspace_bytes, void* stream);

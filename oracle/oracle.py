@@ -47,6 +47,7 @@ def lib() -> ctypes.CDLL:
             "orc_dedisperse_f32": ([_p, _p, _p, _i64, _i64, _i64], _i64),
             "orc_dmt_u8_i32": ([_p, _p, _i64, _i64, _i64, _i64, _p, _i64], None),
             "orc_dmt_f32": ([_p, _p, _i64, _i64, _i64, _i64, _p, _p, _i64], None),
+            "orc_dmt_rowmajor_u8": ([_p, _p, _i64, _i64, _i64, _i64, _p, _i64], None),
             "orc_dmt_roll_f32": ([_p, _p, _i64, _i64, _i64, _p], None),
             "orc_dmt_packed_i32": ([_p, ctypes.c_int, ctypes.c_int, _p, _i64, _i64, _i64, _i64,
                                     _p, _i64], None),
@@ -141,6 +142,17 @@ def dmt(data: np.ndarray, delays: np.ndarray, nchans: int, nsamps: int,
     lib().orc_dmt_f32(_ptr(data), _ptr(delays), ndm, nchans, nsamps, nvalid, _ptr(out),
                       _ptr(out64) if want64 else None, nvalid)
     return (out, out64) if want64 else out
+
+
+def dmt_rowmajor(data_u8: np.ndarray, delays: np.ndarray, nchans: int, nsamps: int,
+                 nvalid: int) -> np.ndarray:
+    """CPU baseline loop (kernels.dedisperse order per DM row, rows in parallel)."""
+    data_u8 = np.ascontiguousarray(data_u8, dtype=np.uint8)
+    delays = np.ascontiguousarray(np.atleast_2d(delays), dtype=np.int32)
+    out = np.zeros((delays.shape[0], nvalid), dtype=np.int32)
+    lib().orc_dmt_rowmajor_u8(_ptr(data_u8), _ptr(delays), delays.shape[0], nchans, nsamps, nvalid,
+                              _ptr(out), nvalid)
+    return out
 
 
 def dmt_packed(packed: np.ndarray, nbits: int, bitorder: str, delays: np.ndarray, nchans: int,

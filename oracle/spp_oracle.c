@@ -176,14 +176,14 @@ void orc_bandpass_u8(const uint8_t* in, int64_t nchans, int64_t nsamps, float* b
     for (int64_t c = 0; c < nchans; ++c) bpass[c] = bpass[c] + (float)in[t * nchans + c];
 }
 
-/* kernels.extract_tim (core/kernels.py:255-278): tim[out_start+t] += sum_c x
- * (float64 accumulator). */
+/* kernels.extract_tim (core/kernels.py:255-278): tim[out_start+t] = sum_c x
+ * (float64 accumulator, stored float32). */
 void orc_collapse_f32(const float* in, int64_t nchans, int64_t nsamps, float* tim,
                       int64_t out_start) {
   for (int64_t t = 0; t < nsamps; ++t) {
     double s = 0.0;
     for (int64_t c = 0; c < nchans; ++c) s += (double)in[t * nchans + c];
-    tim[out_start + t] = (float)((double)tim[out_start + t] + s);
+    tim[out_start + t] = (float)s;
   }
 }
 
@@ -265,5 +265,22 @@ void orc_subband_u8(const uint8_t* in, float* out, const int32_t* delays, const 
     for (int64_t s = 0; s < nsub; ++s) out[t * nsub + s] = 0.f;
     for (int64_t c = 0; c < nchans; ++c)
       out[t * nsub + chan_to_sub[c]] += (float)in[wrap_neg(t + delays[c], nsamps) * nchans + c];
+  }
+}
+
+/* CPU baseline shaped like the reference's parallel path: for each DM row,
+ * kernels.dedisperse's loop order (sample outer, channel inner, float64
+ * accumulator) on unpacked uint8 samples, rows split across threads the way
+ * numba's prange splits work.  Used for the timed CPU baseline only. */
+void orc_dmt_rowmajor_u8(const uint8_t* in, const int32_t* delays, int64_t ndm, int64_t nchans,
+                         int64_t nsamps, int64_t nvalid, int32_t* out, int64_t out_stride) {
+#pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads)
+  for (int64_t i = 0; i < ndm; ++i) {
+    const int32_t* d = delays + i * nchans;
+    for (int64_t t = 0; t < nvalid; ++t) {
+      double s = 0.0;
+      for (int64_t c = 0; c < nchans; ++c) s += in[wrap_neg(t + d[c], nsamps) * nchans + c];
+      out[i * out_stride + t] = (int32_t)s;
+    }
   }
 }

@@ -346,7 +346,20 @@ struct spp_dmt_plan {
   std::vector<int> cands;      // candidate variant indices
   std::vector<int32_t> spans;  // span per candidate
   int cur = 0;                 // index into cands
+  // optional per-kernel timing: events (start, after corner turn, end) per execute
+  bool timing = false;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
 };
+
+static cudaEvent_t plan_event(spp_dmt_plan* p) {
+  if (p->evused == p->evpool.size()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    p->evpool.push_back(e);
+  }
+  return p->evpool[p->evused++];
+}
 
 static int plan_sign(const spp_dmt_plan* p) { return p->mode == SPP_MODE_ROLL ? -1 : 1; }
 
@@ -431,6 +444,7 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
 int spp_dmt_plan_destroy(spp_dmt_plan* p) {
   if (!p) return SPP_OK;
   int rc = SPP_OK;
+  for (cudaEvent_t e : p->evpool) cudaEventDestroy(e);
   if (p->d_delays) rc = cuda_status(cudaFree(p->d_delays), "plan cudaFree");
   delete p;
   return rc;
@@ -493,8 +507,18 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
     return fail(SPP_ERR_UNSUPPORTED, "%lld time tiles exceed the grid limit", (long long)g.ntiles_t);
   const Variant& v = variants()[p->cands[p->cur]];
   void* planar = ws + kStatusBytes;
+  spp_dmt_plan* pm = const_cast<spp_dmt_plan*>(p);
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  if (p->timing) {
+    for (int i = 0; i < 3; ++i) {
+      ev[i] = plan_event(pm);
+      if (!ev[i]) return fail(SPP_ERR_CUDA, "cudaEventCreate failed");
+    }
+    cudaEventRecord(ev[0], st);
+  }
   int rc = launch_corner_turn(p->nbits, in, p->bitorder, p->nchans, nsamps, g, planar, st);
   if (rc) return rc;
+  if (p->timing) cudaEventRecord(ev[1], st);
   DmtArgs a{};
   a.planar = planar;
   a.pitch_w = g.pitch_w;
@@ -514,7 +538,39 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
   a.out_start = out_start;
   a.nvalid = g.nvalid;
   a.status = reinterpret_cast<uint32_t*>(ws);
-  return launch_dmt(v, a, g.ntiles_t, p->ndm, st);
+  rc = launch_dmt(v, a, g.ntiles_t, p->ndm, st);
+  if (rc) return rc;
+  if (p->timing) cudaEventRecord(ev[2], st);
+  return SPP_OK;
+}
+
+int spp_dmt_plan_timing(spp_dmt_plan* p, int enable) {
+  if (!p) return fail(SPP_ERR_ARG, "null plan");
+  p->timing = enable != 0;
+  p->evused = 0;
+  return SPP_OK;
+}
+
+int spp_dmt_plan_timing_read(spp_dmt_plan* p, double* ms_corner_turn, double* ms_dmt,
+                             int32_t* nexec) {
+  if (!p || !ms_corner_turn || !ms_dmt || !nexec) return fail(SPP_ERR_ARG, "null pointer");
+  double a = 0.0, b = 0.0;
+  const size_t n = p->evused / 3;
+  for (size_t i = 0; i < n; ++i) {
+    float x = 0.f, y = 0.f;
+    int rc = cuda_status(cudaEventSynchronize(p->evpool[3 * i + 2]), "event sync");
+    if (rc) return rc;
+    rc = cuda_status(cudaEventElapsedTime(&x, p->evpool[3 * i], p->evpool[3 * i + 1]), "elapsed");
+    if (rc) return rc;
+    rc = cuda_status(cudaEventElapsedTime(&y, p->evpool[3 * i + 1], p->evpool[3 * i + 2]), "elapsed");
+    if (rc) return rc;
+    a += x;
+    b += y;
+  }
+  *ms_corner_turn = a;
+  *ms_dmt = b;
+  *nexec = (int32_t)n;
+  return SPP_OK;
 }
 
 int spp_dmt_execute(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* out,

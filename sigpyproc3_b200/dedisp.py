@@ -155,6 +155,66 @@ class DMTPlan:
     def set_variant(self, v: int) -> None:
         _lib.check(_lib.load().spp_dmt_plan_set_variant(self._h, int(v)))
 
+    def timing(self, enable: bool = True) -> None:
+        """Start (or stop) recording per-kernel CUDA events on each execute."""
+        _lib.check(_lib.load().spp_dmt_plan_timing(self._h, int(enable)))
+
+    def timing_read(self) -> dict:
+        """Summed device milliseconds of the corner turn and the DM-time kernel."""
+        a, b, n = ctypes.c_double(), ctypes.c_double(), ctypes.c_int32()
+        _lib.check(_lib.load().spp_dmt_plan_timing_read(self._h, ctypes.byref(a), ctypes.byref(b),
+                                                        ctypes.byref(n)))
+        return {"ms_corner_turn": a.value, "ms_dmt": b.value, "n": n.value}
+
+    def autotune(self, raw: torch.Tensor, nsamps: int, out: torch.Tensor | None = None,
+                 reps: int = 2, cache: str | None = None) -> dict:
+        """Time every kernel variant on this input and keep the fastest.
+
+        Results are cached per (nbits, nchans, ndm bucket, mode, out dtype) in
+        the JSON file ``cache`` (default ``$SPP_TUNE_CACHE`` or
+        ``~/.cache/sigpyproc3_b200/tuned.json``)."""
+        import json
+        import os
+        from pathlib import Path
+
+        path = Path(cache or os.environ.get("SPP_TUNE_CACHE",
+                                            Path.home() / ".cache/sigpyproc3_b200/tuned.json"))
+        key = (f"nb{self.nbits}-ch{self.nchans}-ndm{1 << max(0, (self.ndm - 1).bit_length())}"
+               f"-{self.mode}-{self.out_dtype}")
+        table = {}
+        if path.exists():
+            try:
+                table = json.loads(path.read_text())
+            except ValueError:
+                table = {}
+        if key in table and 0 <= table[key]["variant"] < self.num_variants:
+            self.set_variant(table[key]["variant"])
+            return table[key]
+        if out is None:
+            out = torch.empty((self.ndm, self.nvalid(nsamps)), dtype=self.out_dtype,
+                              device=raw.device)
+        times = []
+        for v in range(self.num_variants):
+            self.set_variant(v)
+            self.execute(raw, nsamps, out)
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            for _ in range(reps):
+                self.execute(raw, nsamps, out)
+            e.record()
+            e.synchronize()
+            times.append(s.elapsed_time(e) / reps)
+        best = int(np.argmin(times))
+        self.set_variant(best)
+        rec = {"variant": best, "ms": times[best], "all_ms": times, "shape": self.describe()}
+        table[key] = rec
+        try:
+            path.parent.mkdir(parents=True, exist_ok=True)
+            path.write_text(json.dumps(table, indent=1))
+        except OSError:
+            pass
+        return rec
+
     # -- execution --
     def execute(self, raw: torch.Tensor, nsamps: int | None = None, out: torch.Tensor | None = None,
                 out_start: int = 0, stream: torch.cuda.Stream | None = None,
