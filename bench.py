@@ -129,11 +129,18 @@ def _barrier(world):
         dist.barrier()
 
 
-def _workload():
+def _workload(args=None):
+    import dataclasses
+
     from sigpyproc3_b200 import synth
 
     g = synth.C2
-    dms = synth.dm_grid(1000.0, 1024)
+    ndm = 1024
+    if args is not None and (args.nsamps or args.ndm):
+        # reduced case for profiling captures (never a bench value)
+        g = dataclasses.replace(g, nsamps=args.nsamps or g.nsamps)
+        ndm = args.ndm or ndm
+    dms = synth.dm_grid(1000.0, 1024)[np.linspace(0, 1023, ndm).astype(int)]
     delays = np.atleast_2d(g.delays(dms)).astype(np.int32)
     return g, dms, delays
 
@@ -177,10 +184,10 @@ def run_reference(args, rank, world):
     vals = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        vals.append(cpu_sample_run(g, delays, raw_host, threads)["value"])
+        vals.append(cpu_sample_run(g, delays, raw_host, threads, ndm_s=256)["value"])
     wall = time.perf_counter() - t0
     value = float(statistics.mean(vals))
-    sample = "64 of 1024 DM trials (evenly spaced) x 65536 output samples per step, full 4096 channels"
+    sample = "256 of 1024 DM trials (evenly spaced) x 65536 output samples per step, full 4096 channels"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
@@ -200,13 +207,17 @@ def run_gpu(args, rank, world, local):
     from sigpyproc3_b200 import synth
     from sigpyproc3_b200.dedisp import DMTPlan, workspace
 
-    g, dms, delays = _workload()
+    g, dms, delays = _workload(args)
     dev = torch.device("cuda", local)
     raw = synth.c2_filterbank_device(g)
     plan = DMTPlan(delays, g.nchans, g.nsamps, nbits=2, out_dtype=torch.int32)
     nvalid = plan.nvalid(g.nsamps)
     out = torch.empty((delays.shape[0], nvalid), dtype=torch.int32, device=dev)
-    tune = plan.autotune(raw, g.nsamps, out, reps=1, cache=os.environ.get("SPP_TUNE_CACHE"))
+    if args.variant is not None:
+        plan.set_variant(args.variant)
+        tune = {"all_ms": None, "variant": args.variant}
+    else:
+        tune = plan.autotune(raw, g.nsamps, out, reps=1, cache=os.environ.get("SPP_TUNE_CACHE"))
     ws = workspace(plan.workspace_bytes(g.nsamps), dev)
     for _ in range(args.warmup):
         plan.execute(raw, g.nsamps, out, ws=ws)
@@ -279,7 +290,7 @@ def run_gpu(args, rank, world, local):
             threads = os.cpu_count() or 1
             rows = 65536 + int(delays.max())
             rb = g.nchans * g.nbits // 8
-            c = cpu_sample_run(g, delays, host_in.numpy()[: rows * rb], threads)
+            c = cpu_sample_run(g, delays, host_in.numpy()[: rows * rb], threads, ndm_s=256)
             cpu = {"value": c["value"], "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"{c['ndm']} of 1024 DM trials x {c['window']} output samples, "
                              f"{c['seconds']:.1f} s of CPU time"}
@@ -289,7 +300,9 @@ def run_gpu(args, rank, world, local):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u2->int32",
             "data": "synthetic (seeded counter-based generator on device)",
-            "config": {"workload": WORKLOAD, "l2": "inputs larger than L2 (1 GiB in, 4.2 GB out)",
+            "config": {"workload": WORKLOAD if not (args.ndm or args.nsamps) else
+                       f"REDUCED profiling case ndm={args.ndm} nsamps={args.nsamps}",
+                       "l2": "inputs larger than L2 (1 GiB in, 4.2 GB out)",
                        "ndm": int(delays.shape[0]), "nvalid": int(nvalid),
                        "tile": plan.describe(), "autotune_ms": tune.get("all_ms"),
                        "parallelism": f"replicas x{world}"},
@@ -308,6 +321,9 @@ def main():
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--variant", type=int, default=None, help="fix the kernel variant")
+    ap.add_argument("--ndm", type=int, default=None, help="profiling only: fewer DM trials")
+    ap.add_argument("--nsamps", type=int, default=None, help="profiling only: fewer samples")
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

@@ -49,6 +49,7 @@ extern "C" {
 /* output element kinds */
 #define SPP_OUT_F32 0 /* float32 samples                                       */
 #define SPP_OUT_I32 1 /* int32 sums (integer input only; exact)                */
+#define SPP_OUT_U16 2 /* uint16 sums, saturating (subband intermediates)       */
 
 /* delay application modes for the DM-time transform */
 #define SPP_MODE_DEDISPERSE 0 /* out[t] = sum_c x[t + d_c][c]   (kernels.dedisperse) */
@@ -198,6 +199,55 @@ int spp_subband(const void* in, int nbits, int bitorder, int64_t nchans,
                 int64_t nsamps, const int32_t* delays, int32_t maxdelay,
                 const int32_t* chan_to_sub, int64_t nsub, float* out,
                 void* stream);
+
+/* ---- Batched / persistent DM-time transform (many beams, chunks, DM ranges) -------
+ * One persistent launch processes a work list of items; each item is one DM
+ * tile (nrows <= DW trial rows) x one time tile of T samples starting at t0, with
+ * its own planar rows, delay rows and output rows, so beams of different
+ * lengths, channel groups (subbands) and DM ranges share a launch.  Items are
+ * claimed from `counter` (reset by the launch), tiles come from
+ * spp_wl_describe.  Planar rows are produced by spp_corner_turn (layout from
+ * spp_planar_layout) or are the uint16 rows of a previous SPP_OUT_U16 pass
+ * (nbits = 16).  No reference counterpart: the reference runs one DM of one
+ * file per call (kernels.dedisperse, core/kernels.py:340-362). */
+typedef struct spp_dmt_item {
+  const void* planar;     /* first planar row of the channel group           */
+  int64_t pitch_w;        /* 32-bit words per planar row                     */
+  int64_t halo;           /* left halo (samples) of the planar rows          */
+  const int32_t* delays;  /* delay row of the tile's first DM                */
+  int64_t dpitch;         /* elements between delay rows                     */
+  void* out;              /* output row of the tile's first DM               */
+  int64_t out_stride;     /* elements between output rows                    */
+  int64_t out_start;      /* element offset of sample 0 within a row         */
+  int64_t nvalid;         /* samples to write per row                        */
+  int64_t t0;             /* first output sample of this tile                */
+  int32_t nchans;         /* channels in the group                           */
+  int32_t nrows;          /* DM rows in this tile (<= DW)                    */
+  int32_t sign;           /* +1: x[t + d], -1: x[t - d]                      */
+  int32_t dlo, dhi;       /* range of sign*delay (checked on the device)     */
+  int32_t span_max;       /* max over channels of the tile's delay spread    */
+  int32_t out_kind;       /* SPP_OUT_F32 / _I32 / _U16                       */
+  int32_t reserved;
+} spp_dmt_item;           /* 112 bytes */
+
+int spp_wl_num_variants(int nbits, int acc);
+/* cfg[8] = {R, DW, TW, SLAB, STAGES, T (samples per item), threads, samples/word} */
+int spp_wl_describe(int nbits, int acc, int variant, int32_t* cfg);
+int32_t spp_wl_slot_words(int nbits, int acc, int variant, int32_t span_max);
+int64_t spp_wl_smem_bytes(int nbits, int acc, int variant, int32_t slot_w);
+/* nctas <= 0: one wave of resident CTAs.  `items` is a device array. */
+int spp_wl_launch(int nbits, int acc, int variant, const void* items, int32_t nitems,
+                  int32_t slot_w, int32_t* counter, uint32_t* status, int32_t nctas,
+                  void* stream);
+/* CTAs of one resident wave for a variant (sets its shared-memory limit). */
+int32_t spp_wl_default_ctas(int nbits, int acc, int variant, int32_t slot_w);
+/* Planar layout for offsets in [omin, omax] and nvalid outputs tiled by tile_T. */
+int spp_planar_layout(int nbits, int64_t tile_T, int64_t nvalid, int32_t omin,
+                      int32_t omax, int32_t slot_w, int64_t* halo, int64_t* pitch_w);
+/* Raw time-major block -> planar rows (channel-major, time packed in words). */
+int spp_corner_turn(const void* in, int nbits, int bitorder, int64_t nchans,
+                    int64_t nsamps, int64_t halo, void* planar, int64_t pitch_w,
+                    void* stream);
 
 /* ---- Synthetic inputs (benchmark / test data; no reference counterpart) -------
  * Counter-based generators: element i depends only on (seed, start + i)

@@ -26,6 +26,7 @@ BITORDER_BIG = 0
 BITORDER_LITTLE = 1
 OUT_F32 = 0
 OUT_I32 = 1
+OUT_U16 = 2
 MODE_DEDISPERSE = 0
 MODE_ROLL = 1
 ACC_KAHAN32 = 0
@@ -68,6 +69,14 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_boxcar_snr": ([_p, _int, _i64, _i64, _i64, _p, _int, _p, _int, _p, _p, _p, _i64, _p],
                        _int),
     "spp_subband": ([_p, _int, _int, _i64, _i64, _p, _i32, _p, _i64, _p, _p], _int),
+    "spp_wl_num_variants": ([_int, _int], _int),
+    "spp_wl_describe": ([_int, _int, _int, _p], _int),
+    "spp_wl_slot_words": ([_int, _int, _int, _i32], _i32),
+    "spp_wl_smem_bytes": ([_int, _int, _int, _i32], _i64),
+    "spp_wl_launch": ([_int, _int, _int, _p, _i32, _i32, _p, _p, _i32, _p], _int),
+    "spp_wl_default_ctas": ([_int, _int, _int, _i32], _i32),
+    "spp_planar_layout": ([_int, _i64, _i64, _i32, _i32, _i32, _p, _p], _int),
+    "spp_corner_turn": ([_p, _int, _int, _i64, _i64, _i64, _p, _i64, _p], _int),
     "spp_synth_uniform_bytes": ([_p, _i64, _i64, ctypes.c_uint64, _p], _int),
     "spp_synth_gauss_u8": ([_p, _i64, _i64, ctypes.c_uint64, _p, _p], _int),
     "spp_synth_gauss_f32": ([_p, _i64, _i64, ctypes.c_uint64, ctypes.c_float, ctypes.c_float, _p],

@@ -1,0 +1,192 @@
+// Host side of the persistent work-list DM-time kernel (k_dmt_wl) and the
+// exposed corner turn / planar layout used to build batched work.
+#include <algorithm>
+#include <vector>
+
+#include "spp_common.cuh"
+#include "spp_dmt.cuh"
+
+namespace spp {
+
+struct WlVariant {
+  int nb, acc, R, DW, TW, SLAB, STAGES;
+  void (*fn)(const WlArgs);
+};
+
+template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
+static WlVariant mkwl() {
+  return WlVariant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt_wl<NB, R, DW, TW, SLAB, STAGES, ACC>};
+}
+
+#define SPP_WL_INT(NB)                                                                  \
+  mkwl<NB, 2, 8, 1, 64, 3, 0>(), mkwl<NB, 1, 8, 1, 64, 3, 0>(), mkwl<NB, 2, 4, 2, 64, 3, 0>(), \
+      mkwl<NB, 1, 4, 2, 64, 3, 0>()
+
+static const std::vector<WlVariant>& wl_variants() {
+  static const std::vector<WlVariant> v = {
+      SPP_WL_INT(1), SPP_WL_INT(2), SPP_WL_INT(4), SPP_WL_INT(8), SPP_WL_INT(16),
+      mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_KAHAN32>(), mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_KAHAN32>(),
+      mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_F64>(),     mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_F64>(),
+  };
+  return v;
+}
+
+static const WlVariant* wl_find(int nbits, int acc, int variant) {
+  int k = 0;
+  for (const auto& v : wl_variants()) {
+    if (v.nb != nbits || (nbits == 32 && v.acc != acc)) continue;
+    if (k == variant) return &v;
+    ++k;
+  }
+  return nullptr;
+}
+
+static int spw_of_nb(int nb) { return nb == 32 ? 1 : 32 / nb; }
+
+static int64_t wl_T(const WlVariant& v) { return (int64_t)v.TW * 32 * v.R * spw_of_nb(v.nb); }
+
+static int32_t wl_slot(const WlVariant& v, int32_t span) {
+  const int spw = spw_of_nb(v.nb);
+  const int64_t w = wl_T(v) / spw + ceil_div(std::max<int32_t>(span, 0), spw) + 6 + v.R;
+  return (int32_t)round_up(w, 4);
+}
+
+static int64_t wl_smem(const WlVariant& v, int32_t slot_w) {
+  return (int64_t)v.STAGES * dmt_stage_bytes(v.SLAB, slot_w, v.DW) + 16 * v.STAGES + 8 +
+         2 * v.STAGES * 8;
+}
+
+static inline cudaStream_t stq(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+}  // namespace spp
+
+using namespace spp;
+
+extern "C" {
+
+int spp_wl_num_variants(int nbits, int acc) {
+  int n = 0;
+  for (const auto& v : wl_variants())
+    if (v.nb == nbits && (nbits != 32 || v.acc == acc)) ++n;
+  return n;
+}
+
+int spp_wl_describe(int nbits, int acc, int variant, int32_t* cfg) {
+  const WlVariant* v = wl_find(nbits, acc, variant);
+  if (!v || !cfg) return fail(SPP_ERR_ARG, "no work-list variant %d for nbits=%d acc=%d", variant, nbits, acc);
+  cfg[0] = v->R; cfg[1] = v->DW; cfg[2] = v->TW; cfg[3] = v->SLAB; cfg[4] = v->STAGES;
+  cfg[5] = (int32_t)wl_T(*v);
+  cfg[6] = (v->DW * v->TW + 1) * 32;
+  cfg[7] = spw_of_nb(nbits);
+  return SPP_OK;
+}
+
+int32_t spp_wl_slot_words(int nbits, int acc, int variant, int32_t span) {
+  const WlVariant* v = wl_find(nbits, acc, variant);
+  if (!v) return -1;
+  return wl_slot(*v, span);
+}
+
+int64_t spp_wl_smem_bytes(int nbits, int acc, int variant, int32_t slot_w) {
+  const WlVariant* v = wl_find(nbits, acc, variant);
+  if (!v) return -1;
+  return wl_smem(*v, slot_w);
+}
+
+int spp_wl_launch(int nbits, int acc, int variant, const void* items, int32_t nitems,
+                  int32_t slot_w, int32_t* counter, uint32_t* status, int32_t nctas,
+                  void* stream) {
+  const WlVariant* v = wl_find(nbits, acc, variant);
+  if (!v) return fail(SPP_ERR_ARG, "no work-list variant %d for nbits=%d acc=%d", variant, nbits, acc);
+  if (!items || !counter || nitems < 0 || slot_w <= 0 || (slot_w & 3))
+    return fail(SPP_ERR_ARG, "bad work-list arguments");
+  if (nitems == 0) return SPP_OK;
+  const int64_t smem = wl_smem(*v, slot_w);
+  if (smem > 227 * 1024) return fail(SPP_ERR_UNSUPPORTED, "work list needs %lld B shared memory", (long long)smem);
+  cudaStream_t st = stq(stream);
+  int rc = SPP_OK;
+  if (smem > 48 * 1024) {
+    rc = set_smem_attr(reinterpret_cast<const void*>(v->fn), smem);
+    if (rc) return rc;
+  }
+  const int threads = (v->DW * v->TW + 1) * 32;
+  if (nctas <= 0) {
+    int dev = 0, sms = 0, per = 0;
+    rc = cuda_status(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    rc = cuda_status(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+    if (rc) return rc;
+    rc = cuda_status(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, v->fn, threads, smem), "occupancy");
+    if (rc) return rc;
+    nctas = std::max(1, sms * std::max(per, 1));
+  }
+  nctas = std::min<int32_t>(nctas, nitems);
+  rc = cuda_status(cudaMemsetAsync(counter, 0, sizeof(int32_t), st), "counter reset");
+  if (rc) return rc;
+  WlArgs w{};
+  w.items = static_cast<const DmtItem*>(items);
+  w.nitems = nitems;
+  w.slot_w = slot_w;
+  w.counter = counter;
+  w.status = status;
+  v->fn<<<nctas, threads, smem, st>>>(w);
+  return cuda_status(cudaGetLastError(), "work-list launch");
+}
+
+int spp_planar_layout(int nbits, int64_t tile_T, int64_t nvalid, int32_t omin, int32_t omax,
+                      int32_t slot_w, int64_t* halo, int64_t* pitch_w) {
+  if (!halo || !pitch_w || tile_T <= 0 || slot_w <= 0) return fail(SPP_ERR_ARG, "bad layout arguments");
+  if (nbits != 1 && nbits != 2 && nbits != 4 && nbits != 8 && nbits != 16 && nbits != 32)
+    return fail(SPP_ERR_ARG, "bad nbits %d", nbits);
+  const int spw = spw_of_nb(nbits);
+  *halo = round_up(std::max<int64_t>(0, -(int64_t)omin), 4 * spw);
+  const int64_t ntiles = ceil_div(std::max<int64_t>(nvalid, 1), tile_T);
+  const int64_t last = ntiles * tile_T + std::max<int64_t>(0, omax) + *halo;
+  *pitch_w = round_up(ceil_div(last, spw) + slot_w + 8, 4);
+  return SPP_OK;
+}
+
+int spp_corner_turn(const void* in, int nbits, int bitorder, int64_t nchans, int64_t nsamps,
+                    int64_t halo, void* planar, int64_t pitch_w, void* stream) {
+  if (!in || !planar) return fail(SPP_ERR_ARG, "null pointer");
+  if (nbits != 1 && nbits != 2 && nbits != 4 && nbits != 8 && nbits != 32)
+    return fail(SPP_ERR_ARG, "bad nbits %d", nbits);
+  if (nchans <= 0 || nsamps <= 0 || pitch_w <= 0 || (pitch_w & 3) || halo < 0)
+    return fail(SPP_ERR_ARG, "bad shape");
+  if (nbits < 8 && (nchans * nbits) % 8) return fail(SPP_ERR_ARG, "nchans*nbits must be a multiple of 8");
+  cudaStream_t st = stq(stream);
+  if (nbits == 32) {
+    dim3 grid((unsigned)ceil_div(nchans, 32), (unsigned)std::min<int64_t>(ceil_div(pitch_w, 32), 65535));
+    k_corner_turn_f32<<<grid, 256, 0, st>>>(static_cast<const float*>(in), nchans, nsamps, halo,
+                                            static_cast<float*>(planar), pitch_w, nullptr, nullptr,
+                                            nullptr);
+  } else {
+    dim3 grid((unsigned)ceil_div(nchans, kCtChans),
+              (unsigned)std::min<int64_t>(ceil_div(pitch_w, kCtWords), 65535));
+    const uint8_t* raw = static_cast<const uint8_t*>(in);
+    uint32_t* pl = static_cast<uint32_t*>(planar);
+    switch (nbits) {
+      case 1: k_corner_turn_int<1><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w); break;
+      case 2: k_corner_turn_int<2><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w); break;
+      case 4: k_corner_turn_int<4><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w); break;
+      default: k_corner_turn_int<8><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w); break;
+    }
+  }
+  return cuda_status(cudaGetLastError(), "corner turn launch");
+}
+
+}  // extern "C"
+
+extern "C" int32_t spp_wl_default_ctas(int nbits, int acc, int variant, int32_t slot_w) {
+  const WlVariant* v = wl_find(nbits, acc, variant);
+  if (!v) return -1;
+  int dev = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+  const int64_t smem = wl_smem(*v, slot_w);
+  if (smem > 48 * 1024 && set_smem_attr(reinterpret_cast<const void*>(v->fn), smem)) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, v->fn, (v->DW * v->TW + 1) * 32, smem) !=
+      cudaSuccess)
+    return -1;
+  return std::max(1, sms * std::max(per, 1));
+}

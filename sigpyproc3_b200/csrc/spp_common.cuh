@@ -16,6 +16,8 @@ namespace spp {
 int fail(int code, const char* fmt, ...);
 // Maps a CUDA error to SPP_ERR_CUDA with context; SPP_OK if e == cudaSuccess.
 int cuda_status(cudaError_t e, const char* what);
+// Sets cudaFuncAttributeMaxDynamicSharedMemorySize once per (device, kernel).
+int set_smem_attr(const void* fn, int64_t bytes);
 
 static inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 static inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }

@@ -4,7 +4,9 @@
 #include <atomic>
 #include <climits>
 #include <cstring>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <vector>
 
 #include "spp_common.cuh"
@@ -28,6 +30,25 @@ int cuda_status(cudaError_t e, const char* what) {
 }
 
 static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Raises a kernel's dynamic shared memory limit once per (device, kernel):
+// later calls with a size at or below the recorded one issue no CUDA call, so
+// launches stay legal inside CUDA-graph capture after one eager run.
+int set_smem_attr(const void* fn, int64_t bytes) {
+  static std::mutex mu;
+  static std::vector<std::tuple<int, const void*, int64_t>> done;
+  int dev = 0;
+  int rc = cuda_status(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(mu);
+  for (auto& e : done)
+    if (std::get<0>(e) == dev && std::get<1>(e) == fn && std::get<2>(e) >= bytes) return SPP_OK;
+  rc = cuda_status(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                   "cudaFuncSetAttribute");
+  if (rc) return rc;
+  done.emplace_back(dev, fn, bytes);
+  return SPP_OK;
+}
 
 static inline bool valid_nbits(int nbits) {
   return nbits == 1 || nbits == 2 || nbits == 4 || nbits == 8 || nbits == 32;
@@ -55,12 +76,21 @@ struct Variant {
   int nb, acc, R, DW, TW, SLAB, STAGES;
   void (*fn)(const DmtArgs);
   int single;  // 1: meant for one DM (time-split warps)
+  int planes;  // 1: bit-sliced kernel over bit-plane rows (R = words per thread)
 };
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
 static Variant mk(int single) {
   return Variant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt<NB, R, DW, TW, SLAB, STAGES, ACC>,
-                 single};
+                 single, 0};
+}
+
+// Bit-sliced counters hold sums below 2^kBitLevels.
+constexpr int kBitLevels = 14;
+
+template <int NB, int P, int DW, int TW, int STAGES>
+static Variant mkb() {
+  return Variant{NB, 0, P, DW, TW, 64, STAGES, &k_dmt_bits<NB, P, DW, TW, STAGES, kBitLevels>, 0, 1};
 }
 
 #define SPP_INT_VARIANTS(NB)                    \
@@ -69,6 +99,9 @@ static Variant mk(int single) {
 
 static const std::vector<Variant>& variants() {
   static const std::vector<Variant> v = {
+      // bit-sliced (1- and 2-bit data)
+      mkb<2, 2, 8, 1, 2>(), mkb<2, 1, 8, 1, 3>(), mkb<2, 2, 16, 1, 2>(), mkb<2, 2, 4, 2, 2>(),
+      mkb<1, 2, 8, 1, 2>(), mkb<1, 1, 8, 1, 3>(), mkb<1, 2, 16, 1, 2>(),
       SPP_INT_VARIANTS(1),
       SPP_INT_VARIANTS(2),
       SPP_INT_VARIANTS(4),
@@ -90,17 +123,19 @@ static const std::vector<Variant>& variants() {
 }
 
 static inline int spw_of(int nb) { return nb == 32 ? 1 : 32 / nb; }
+static inline int spw_v(const Variant& v) { return v.planes ? 32 : spw_of(v.nb); }
 static inline int64_t tile_T(const Variant& v) {
-  return (int64_t)v.TW * 32 * v.R * spw_of(v.nb);
+  return (int64_t)v.TW * 32 * v.R * spw_v(v);
 }
 
 static int slot_words(const Variant& v, int32_t span) {
-  const int spw = spw_of(v.nb);
+  const int spw = spw_v(v);
   const int64_t w = tile_T(v) / spw + ceil_div(std::max<int32_t>(span, 0), spw) + 6 + v.R;
   return (int)round_up(w, 4);
 }
 
 static int64_t smem_bytes(const Variant& v, int slot_w) {
+  if (v.planes) return v.STAGES * bits_stage_bytes(v.nb, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
   return v.STAGES * dmt_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
 }
 
@@ -108,6 +143,7 @@ static constexpr int64_t kMaxSmem = 227 * 1024;
 
 // Planar geometry for one execution.
 struct Geometry {
+  int planes;
   int spw;
   int64_t halo;     // samples
   int64_t pitch_w;  // words per channel row
@@ -120,13 +156,14 @@ struct Geometry {
 static Geometry geometry(const Variant& v, int64_t nchans, int64_t nsamps, int64_t nvalid,
                          int32_t omin, int32_t omax, int slot_w) {
   Geometry g{};
-  g.spw = spw_of(v.nb);
+  g.planes = v.planes;
+  g.spw = spw_v(v);
   g.nvalid = nvalid;
   g.halo = round_up(std::max<int64_t>(0, -(int64_t)omin), 4 * g.spw);
   g.ntiles_t = ceil_div(std::max<int64_t>(nvalid, 1), tile_T(v));
   const int64_t last = g.ntiles_t * tile_T(v) + std::max<int64_t>(0, omax) + g.halo;
   g.pitch_w = round_up(ceil_div(last, g.spw) + slot_w + 8, 4);
-  g.bytes = nchans * g.pitch_w * 4;
+  g.bytes = nchans * (v.planes ? v.nb : 1) * g.pitch_w * 4;
   (void)nsamps;
   return g;
 }
@@ -135,11 +172,7 @@ static int ensure_smem(const Variant& v, int64_t bytes) {
   if (bytes > kMaxSmem)
     return fail(SPP_ERR_UNSUPPORTED, "DM tile needs %lld B of shared memory (> %lld)",
                 (long long)bytes, (long long)kMaxSmem);
-  if (bytes > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(reinterpret_cast<const void*>(v.fn),
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute");
-  }
+  if (bytes > 48 * 1024) return set_smem_attr(reinterpret_cast<const void*>(v.fn), bytes);
   return SPP_OK;
 }
 
@@ -147,7 +180,18 @@ static int launch_corner_turn(int nb, const void* in, int bitorder, int64_t ncha
                               int64_t nsamps, const Geometry& g, void* planar, cudaStream_t st,
                               const double* zdm = nullptr, const float* chanwts = nullptr,
                               const float* bpass = nullptr) {
-  if (nb == 32) {
+  if (g.planes) {
+    dim3 grid((unsigned)ceil_div(nchans, kCtChans),
+              (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, kCtWords), 65535));
+    const uint8_t* raw = static_cast<const uint8_t*>(in);
+    uint32_t* pl = static_cast<uint32_t*>(planar);
+    if (nb == 1)
+      k_corner_turn_planes<1><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, g.halo, pl, g.pitch_w);
+    else if (nb == 2)
+      k_corner_turn_planes<2><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, g.halo, pl, g.pitch_w);
+    else
+      return fail(SPP_ERR_UNSUPPORTED, "bit planes for nbits=%d", nb);
+  } else if (nb == 32) {
     dim3 grid((unsigned)ceil_div(nchans, 32),
               (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, 32), 65535));
     k_corner_turn_f32<<<grid, 256, 0, st>>>(static_cast<const float*>(in), nchans, nsamps,
@@ -410,6 +454,7 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
     const Variant& v = vs[i];
     if (v.nb != nbits || (nbits == 32 && v.acc != acc)) continue;
     if (ndm == 1 ? !v.single : v.single) continue;
+    if (v.planes && nchans * ((1 << nbits) - 1) >= (1 << kBitLevels)) continue;
     // span for tiles of v.DW consecutive DMs
     int32_t span = 0;
     for (int64_t d0 = 0; d0 < ndm; d0 += v.DW) {

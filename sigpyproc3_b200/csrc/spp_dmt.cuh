@@ -29,7 +29,8 @@ namespace spp {
 template <int NB>
 struct Pack {
   static constexpr int kSpw = (NB == 32) ? 1 : 32 / NB;         // samples per word
-  static constexpr int kLogSpw = (NB == 32) ? 0 : (NB == 1 ? 5 : NB == 2 ? 4 : NB == 4 ? 3 : 2);
+  static constexpr int kLogSpw =
+      (NB == 32) ? 0 : (NB == 1 ? 5 : NB == 2 ? 4 : NB == 4 ? 3 : NB == 8 ? 2 : 1);
   static constexpr uint32_t kMaskByte = (NB == 1)   ? 0x01010101u
                                         : (NB == 2) ? 0x03030303u
                                         : (NB == 4) ? 0x0F0F0F0Fu
@@ -210,7 +211,10 @@ struct IntAcc {
     }
   }
   __device__ __forceinline__ void add(uint32_t v, int k) {
-    if (NB == 8) {
+    if (NB == 16) {
+      S[k][0] += v & 0xFFFFu;
+      S[k][1] += v >> 16;
+    } else if (NB == 8) {
       E[k][0] += v & 0x00FF00FFu;
       O[k][0] += (v >> 8) & 0x00FF00FFu;
     } else {
@@ -219,7 +223,7 @@ struct IntAcc {
     }
   }
   __device__ __forceinline__ void flush8() {
-    if (NB == 8) return;
+    if (NB >= 8) return;
 #pragma unroll
     for (int k = 0; k < R; ++k)
 #pragma unroll
@@ -230,6 +234,7 @@ struct IntAcc {
       }
   }
   __device__ __forceinline__ void flush16() {
+    if (NB == 16) return;
 #pragma unroll
     for (int k = 0; k < R; ++k)
 #pragma unroll
@@ -415,7 +420,7 @@ k_dmt(const DmtArgs a) {
     acc.zero();
     constexpr int K16 = (P::kCap16 / SLAB) > 0 ? (P::kCap16 / SLAB) : 1;
     constexpr int F8 = (P::kCap8 >= SLAB) ? SLAB : 16;  // byte-lane flush period (channels)
-    static_assert(NB == 8 || P::kCap8 >= F8, "byte lanes would overflow");
+    static_assert(NB >= 8 || P::kCap8 >= F8, "byte lanes would overflow");
     static_assert(NB != 8 || P::kCap16 >= SLAB, "16-bit lanes would overflow");
     for (int k = 0; k < nslab; ++k) {
       const int s = k % STAGES;
@@ -446,7 +451,16 @@ k_dmt(const DmtArgs a) {
     acc.flush16();
     if (!ok || dm >= a.ndm) return;
     const int64_t tb = t0 + tloc;
-    if (a.out_kind == SPP_OUT_I32) {
+    if (a.out_kind == SPP_OUT_U16) {
+      uint16_t* out = static_cast<uint16_t*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int j = 0; j < SPW; ++j) {
+          const int64_t t = tb + r * SPW + j;
+          if (t < a.nvalid) out[t] = (uint16_t)min(acc.S[r][j], 65535u);
+        }
+    } else if (a.out_kind == SPP_OUT_I32) {
       int32_t* out = static_cast<int32_t*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
 #pragma unroll
       for (int r = 0; r < R; ++r)
@@ -468,4 +482,641 @@ k_dmt(const DmtArgs a) {
   }
 }
 
+
+// ----------------------------------------------------------------------------
+// Persistent work-list DM-time kernel.  Each work item is one DM tile (up to
+// DW rows) x one time tile of one (beam, channel group) with its own planar
+// rows, delay rows and output rows, so uneven beams, chunk lengths and DM
+// ranges run in a single launch.  CTAs stay resident (grid = a few per SM);
+// the producer warp claims items from a global counter and streams their
+// channel slabs through the STAGES-deep ring, tagging every stage with the
+// item index; consumers follow the tags, so the ring never drains between
+// items.  A tag of -1 ends the CTA.
+// ----------------------------------------------------------------------------
+struct DmtItem {
+  const void* planar;     // first planar row of the channel group
+  int64_t pitch_w;        // words per planar row
+  int64_t halo;           // samples of left halo in the planar rows
+  const int32_t* delays;  // delay row of the tile's first DM (rows dpitch apart)
+  int64_t dpitch;
+  void* out;              // output row of the tile's first DM
+  int64_t out_stride;     // elements between output rows
+  int64_t out_start;      // element offset of sample 0 in a row
+  int64_t nvalid;         // samples to write per row
+  int64_t t0;             // first output sample of the tile
+  int32_t nchans;         // channels in the group
+  int32_t nrows;          // DM rows in the tile (<= DW)
+  int32_t sign;
+  int32_t dlo, dhi;       // declared range of sign*delay
+  int32_t span_max;
+  int32_t out_kind;
+  int32_t reserved;
+};
+static_assert(sizeof(DmtItem) == 112, "DmtItem layout is part of the C ABI");
+
+struct WlArgs {
+  const DmtItem* items;
+  int32_t nitems;
+  int32_t slot_w;
+  int32_t* counter;  // zeroed before the launch
+  uint32_t* status;
+};
+
+template <int NB, int R, int SPW>
+__device__ __forceinline__ void store_int_outputs(const IntAcc<NB, R>& acc, const DmtItem& it,
+                                                  int row, int64_t tb) {
+  if (it.out_kind == SPP_OUT_U16) {
+    uint16_t* out = static_cast<uint16_t*>(it.out) + (int64_t)row * it.out_stride + it.out_start;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int j = 0; j < SPW; ++j) {
+        const int64_t t = tb + r * SPW + j;
+        if (t < it.nvalid) out[t] = (uint16_t)min(acc.S[r][j], 65535u);
+      }
+  } else if (it.out_kind == SPP_OUT_I32) {
+    int32_t* out = static_cast<int32_t*>(it.out) + (int64_t)row * it.out_stride + it.out_start;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int j = 0; j < SPW; ++j) {
+        const int64_t t = tb + r * SPW + j;
+        if (t < it.nvalid) out[t] = (int32_t)acc.S[r][j];
+      }
+  } else {
+    float* out = static_cast<float*>(it.out) + (int64_t)row * it.out_stride + it.out_start;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int j = 0; j < SPW; ++j) {
+        const int64_t t = tb + r * SPW + j;
+        if (t < it.nvalid) out[t] = (float)acc.S[r][j];
+      }
+  }
+}
+
+template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
+__global__ void __launch_bounds__(DmtShape<NB, R, DW, TW, SLAB, STAGES>::kThreads)
+k_dmt_wl(const WlArgs w) {
+  using Sh = DmtShape<NB, R, DW, TW, SLAB, STAGES>;
+  using P = Pack<NB>;
+  constexpr int SPW = P::kSpw;
+  constexpr int NWC = Sh::kNwc;
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
+  int32_t* sdel = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * w.slot_w);
+  int32_t* sbase = sdel + STAGES * DW * SLAB;
+  int32_t* stag = sbase + STAGES * SLAB;  // per stage: item, slab, nslab, pad
+  uint64_t* full = reinterpret_cast<uint64_t*>(stag + 4 * STAGES);
+  uint64_t* empty = full + STAGES;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NWC);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == NWC) {
+    // ---------------- producer warp ----------------
+    uint32_t gk = 0;
+    bool ok = true;
+    while (ok) {
+      int it_idx = 0;
+      if (lane == 0) it_idx = atomicAdd(w.counter, 1);
+      it_idx = __shfl_sync(0xffffffffu, it_idx, 0);
+      if (it_idx >= w.nitems) break;
+      const DmtItem it = w.items[it_idx];
+      const uint32_t* planar = static_cast<const uint32_t*>(it.planar);
+      const int nslab = (it.nchans + SLAB - 1) / SLAB;
+      for (int k = 0; k < nslab; ++k, ++gk) {
+        const int s = gk % STAGES;
+        if (gk >= STAGES && !mbar_wait(&empty[s], ((gk / STAGES) - 1) & 1, w.status)) {
+          ok = false;
+          break;
+        }
+        const int c0 = k * SLAB;
+        const int nc = min(SLAB, it.nchans - c0);
+        int64_t ws_reg[(SLAB + 31) / 32];
+#pragma unroll
+        for (int jj = 0; jj < (SLAB + 31) / 32; ++jj) {
+          const int j = lane + jj * 32;
+          ws_reg[jj] = 0;
+          if (j < nc) {
+            const int c = c0 + j;
+            int32_t dv[DW];
+            int32_t mn = INT32_MAX, mx = INT32_MIN;
+#pragma unroll
+            for (int i = 0; i < DW; ++i) {
+              const int r = min(i, it.nrows - 1);
+              int32_t d = it.sign * __ldg(it.delays + (int64_t)r * it.dpitch + c);
+              if (d < it.dlo || d > it.dhi) {
+                dev_flag(w.status, SPP_DEV_RANGE, (uint32_t)c);
+                d = min(max(d, it.dlo), it.dhi);
+              }
+              dv[i] = d;
+              mn = min(mn, d);
+              mx = max(mx, d);
+            }
+            if (mx - mn > it.span_max) {
+              dev_flag(w.status, SPP_DEV_RANGE, (uint32_t)c | 0x80000000u);
+              mx = mn + it.span_max;
+            }
+#pragma unroll
+            for (int i = 0; i < DW; ++i) sdel[(s * DW + i) * SLAB + j] = min(dv[i], mx);
+            const int64_t ws = ((it.t0 + mn + it.halo) / SPW) & ~int64_t(3);
+            sbase[s * SLAB + j] = (int32_t)(ws * SPW - it.halo - it.t0);
+            ws_reg[jj] = ws;
+          }
+        }
+        if (lane == 0) {
+          stag[4 * s + 0] = it_idx;
+          stag[4 * s + 1] = k;
+          stag[4 * s + 2] = nslab;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(&full[s], (uint32_t)nc * w.slot_w * 4u);
+        __syncwarp();
+#pragma unroll
+        for (int jj = 0; jj < (SLAB + 31) / 32; ++jj) {
+          const int j = lane + jj * 32;
+          if (j < nc)
+            bulk_g2s(sdata + ((int64_t)s * SLAB + j) * w.slot_w,
+                     planar + (int64_t)(c0 + j) * it.pitch_w + ws_reg[jj], w.slot_w * 4u, &full[s]);
+        }
+      }
+    }
+    if (ok) {
+      const int s = gk % STAGES;
+      if (gk < STAGES || mbar_wait(&empty[s], ((gk / STAGES) - 1) & 1, w.status)) {
+        if (lane == 0) {
+          stag[4 * s + 0] = -1;
+          mbar_arrive(&full[s]);
+        }
+      }
+    }
+    return;
+  }
+
+  // ---------------- consumer warps ----------------
+  const int dmw = warp / TW, tw = warp % TW;
+  const int tloc = tw * (32 * R * SPW) + lane * (R * SPW);
+  uint32_t gk = 0;
+  if constexpr (NB == 32) {
+    float s_acc[R], c_acc[R];
+    double d_acc[R];
+    DmtItem it{};
+    for (;; ++gk) {
+      const int s = gk % STAGES;
+      if (!mbar_wait(&full[s], (gk / STAGES) & 1, w.status)) return;
+      const int it_idx = stag[4 * s + 0];
+      if (it_idx < 0) return;
+      const int k = stag[4 * s + 1], nslab = stag[4 * s + 2];
+      if (k == 0) {
+        it = w.items[it_idx];
+#pragma unroll
+        for (int r = 0; r < R; ++r) { s_acc[r] = 0.f; c_acc[r] = 0.f; d_acc[r] = 0.0; }
+      }
+      const int nc = min(SLAB, it.nchans - k * SLAB);
+      const float* sd = reinterpret_cast<const float*>(sdata) + (int64_t)s * SLAB * w.slot_w;
+      const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
+      const int32_t* bs = sbase + s * SLAB;
+#pragma unroll 4
+      for (int j = 0; j < nc; ++j) {
+        const float* row = sd + j * w.slot_w + (tloc + dl[j] - bs[j]);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float x = row[r];
+          if (ACC == SPP_ACC_F64) {
+            d_acc[r] += (double)x;
+          } else {
+            const float y = __fsub_rn(x, c_acc[r]);
+            const float t = __fadd_rn(s_acc[r], y);
+            c_acc[r] = __fsub_rn(__fsub_rn(t, s_acc[r]), y);
+            s_acc[r] = t;
+          }
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+      if (k == nslab - 1 && dmw < it.nrows) {
+        float* out = static_cast<float*>(it.out) + (int64_t)dmw * it.out_stride + it.out_start;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int64_t t = it.t0 + tloc + r;
+          if (t < it.nvalid)
+            out[t] = (ACC == SPP_ACC_F64) ? (float)d_acc[r] : __fsub_rn(s_acc[r], c_acc[r]);
+        }
+      }
+    }
+  } else {
+    IntAcc<NB, R> acc;
+    acc.zero();
+    constexpr int K16 = (P::kCap16 / SLAB) > 0 ? (P::kCap16 / SLAB) : 1;
+    constexpr int F8 = (P::kCap8 >= SLAB) ? SLAB : 16;
+    DmtItem it{};
+    for (;; ++gk) {
+      const int s = gk % STAGES;
+      if (!mbar_wait(&full[s], (gk / STAGES) & 1, w.status)) return;
+      const int it_idx = stag[4 * s + 0];
+      if (it_idx < 0) return;
+      const int k = stag[4 * s + 1], nslab = stag[4 * s + 2];
+      if (k == 0) {
+        it = w.items[it_idx];
+        acc.zero();
+      }
+      const int nc = min(SLAB, it.nchans - k * SLAB);
+      const uint32_t* sd = sdata + (int64_t)s * SLAB * w.slot_w;
+      const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
+      const int32_t* bs = sbase + s * SLAB;
+      for (int jb = 0; jb < nc; jb += F8) {
+        const int je = min(nc, jb + F8);
+#pragma unroll 4
+        for (int j = jb; j < je; ++j) {
+          const int o = tloc + dl[j] - bs[j];
+          const uint32_t* row = sd + j * w.slot_w + (o >> P::kLogSpw);
+          const int sh = (o & (SPW - 1)) * NB;
+          uint32_t wv[R + 1];
+#pragma unroll
+          for (int r = 0; r <= R; ++r) wv[r] = row[r];
+#pragma unroll
+          for (int r = 0; r < R; ++r) acc.add(__funnelshift_r(wv[r], wv[r + 1], sh), r);
+        }
+        acc.flush8();
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+      if (((k + 1) % K16) == 0) acc.flush16();
+      if (k == nslab - 1) {
+        acc.flush16();
+        if (dmw < it.nrows) store_int_outputs<NB, R, SPW>(acc, it, dmw, it.t0 + tloc);
+      }
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// Bit-sliced DM-time kernel for 1- and 2-bit data.
+//
+// Planar "plane rows": row c*NB + k holds bit k of channel c's samples, 32
+// samples per word (LSB first).  A thread owns P words of time, interleaved
+// across the warp (word = lane + 32*p, so a warp's loads hit 32 consecutive
+// words: no bank conflicts).  Per channel it funnel-shifts each plane word to
+// its delay and adds it, with weight 2^k, into a bit-sliced counter: word
+// A[p][l] holds bit l of the 32 running sums.  Additions go through
+// carry-save adders (three words in, sum and carry out; the carry-save
+// popcount of Harley & Seal, as in Mula, Kurz & Lemire 2018), with at most
+// one pending word per level, so a channel costs about four LOP3s per plane
+// word.  The pending pattern over a full 64-channel slab is fixed, so the
+// compiler resolves it statically.  L levels hold counts up to 2^L - 1.
+// ----------------------------------------------------------------------------
+// Carry-save adder: acc <- acc ^ x ^ y, carry <- majority(acc, x, y).
+__device__ __forceinline__ void csa(uint32_t& acc, uint32_t x, uint32_t y, uint32_t& carry) {
+  const uint32_t a = acc;
+  acc = a ^ x ^ y;
+  carry = (a & x) | (a & y) | (x & y);
+}
+// Half adder: acc <- acc ^ x, carry <- acc & x.
+__device__ __forceinline__ void half(uint32_t& acc, uint32_t x, uint32_t& carry) {
+  carry = acc & x;
+  acc ^= x;
+}
+
+// Bit-sliced counter of 32 sums per word position p: A[p][l] holds bit l.
+// Inputs arrive as four channels at a time (one word per plane and p); a
+// fixed network of carry-save adders folds them in (levels 0..3 per four
+// channels, 4..5 per sixteen, 6..7 per sixty-four) and the single carry that
+// leaves each 64-channel slab ripples through the top levels with half adders.
+template <int P, int L>
+struct BitCounter {
+  uint32_t A[P][L];
+
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int p = 0; p < P; ++p)
+#pragma unroll
+      for (int l = 0; l < L; ++l) A[p][l] = 0u;
+  }
+  // Four channels of 2-bit samples: lo[q] weight 1, hi[q] weight 2.  Returns
+  // (through out) the weight-16 carry word.
+  __device__ __forceinline__ void quad2(int p, const uint32_t (&lo)[4], const uint32_t (&hi)[4],
+                                        uint32_t& out16) {
+    uint32_t ta, tb, fa, fb, fc, ea, eb;
+    csa(A[p][0], lo[0], lo[1], ta);
+    csa(A[p][0], lo[2], lo[3], tb);
+    csa(A[p][1], hi[0], hi[1], fa);
+    csa(A[p][1], hi[2], hi[3], fb);
+    csa(A[p][1], ta, tb, fc);
+    csa(A[p][2], fa, fb, ea);
+    half(A[p][2], fc, eb);
+    csa(A[p][3], ea, eb, out16);
+  }
+  // Four channels of 1-bit samples.  Returns the weight-4 carry word.
+  __device__ __forceinline__ void quad1(int p, const uint32_t (&x)[4], uint32_t& out4) {
+    uint32_t ta, tb;
+    csa(A[p][0], x[0], x[1], ta);
+    csa(A[p][0], x[2], x[3], tb);
+    csa(A[p][1], ta, tb, out4);
+  }
+  // Four words of weight 2^l -> accumulate at level l, l+1; carry of weight 2^(l+2).
+  __device__ __forceinline__ void fold4(int p, int l, const uint32_t (&w)[4], uint32_t& out) {
+    uint32_t a, b;
+    csa(A[p][l], w[0], w[1], a);
+    csa(A[p][l], w[2], w[3], b);
+    csa(A[p][l + 1], a, b, out);
+  }
+  // Ripple a carry word of weight 2^l through the remaining levels.
+  __device__ __forceinline__ void ripple(int p, int l, uint32_t c) {
+#pragma unroll
+    for (int k = 0; k < L; ++k) {
+      if (k < l) continue;
+      uint32_t nc;
+      half(A[p][k], c, nc);
+      c = nc;
+    }
+  }
+  __device__ __forceinline__ uint32_t count(int p, int i) const {
+    uint32_t v = 0;
+#pragma unroll
+    for (int l = 0; l < L; ++l) v |= ((A[p][l] >> i) & 1u) << l;
+    return v;
+  }
+};
+
+template <int NB, int P, int DW, int TW, int STAGES>
+struct BitsShape {
+  static constexpr int kSlab = 64;
+  static constexpr int kNwc = DW * TW;
+  static constexpr int kThreads = (kNwc + 1) * 32;
+  static constexpr int kT = TW * 32 * P * 32;  // samples per CTA tile
+};
+
+__host__ __device__ constexpr int64_t bits_stage_bytes(int nb, int slot_w, int dw) {
+  return (int64_t)64 * nb * slot_w * 4 + (int64_t)dw * 64 * 4 + 64 * 4;
+}
+
+template <int NB, int P, int DW, int TW, int STAGES, int L>
+__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, STAGES>::kThreads)
+k_dmt_bits(const DmtArgs a) {
+  using Sh = BitsShape<NB, P, DW, TW, STAGES>;
+  constexpr int SLAB = Sh::kSlab;
+  constexpr int NWC = Sh::kNwc;
+  constexpr int T = Sh::kT;
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
+  int32_t* sdel = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * NB * a.slot_w);
+  int32_t* sbase = sdel + STAGES * DW * SLAB;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sbase + STAGES * SLAB);
+  uint64_t* empty = full + STAGES;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int dm0 = blockIdx.x * DW;
+  const int64_t t0 = (int64_t)blockIdx.y * T;
+  const int nslab = (a.nchans + SLAB - 1) / SLAB;
+
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NWC);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == NWC) {
+    const uint32_t* planar = static_cast<const uint32_t*>(a.planar);
+    for (int k = 0; k < nslab; ++k) {
+      const int s = k % STAGES;
+      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1, a.status)) break;
+      const int c0 = k * SLAB;
+      const int nc = min(SLAB, a.nchans - c0);
+      int64_t ws_reg[2];
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj) {
+        const int j = lane + jj * 32;
+        ws_reg[jj] = 0;
+        if (j < nc) {
+          const int c = c0 + j;
+          int32_t dv[DW];
+          int32_t mn = INT32_MAX, mx = INT32_MIN;
+#pragma unroll
+          for (int i = 0; i < DW; ++i) {
+            const int dm = min(dm0 + i, a.ndm - 1);
+            int32_t d = a.sign * __ldg(a.delays + (int64_t)dm * a.dpitch + c);
+            if (d < a.dlo || d > a.dhi) {
+              dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)c);
+              d = min(max(d, a.dlo), a.dhi);
+            }
+            dv[i] = d;
+            mn = min(mn, d);
+            mx = max(mx, d);
+          }
+          if (mx - mn > a.span_max) {
+            dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)c | 0x80000000u);
+            mx = mn + a.span_max;
+          }
+#pragma unroll
+          for (int i = 0; i < DW; ++i) sdel[(s * DW + i) * SLAB + j] = min(dv[i], mx);
+          const int64_t ws = ((t0 + mn + a.halo) / 32) & ~int64_t(3);
+          sbase[s * SLAB + j] = (int32_t)(ws * 32 - a.halo - t0);
+          ws_reg[jj] = ws;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive_expect_tx(&full[s], (uint32_t)nc * NB * a.slot_w * 4u);
+      __syncwarp();
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj) {
+        const int j = lane + jj * 32;
+        if (j < nc) {
+#pragma unroll
+          for (int b = 0; b < NB; ++b)
+            bulk_g2s(sdata + (((int64_t)s * SLAB + j) * NB + b) * a.slot_w,
+                     planar + ((int64_t)(c0 + j) * NB + b) * a.pitch_w + ws_reg[jj],
+                     a.slot_w * 4u, &full[s]);
+        }
+      }
+    }
+    return;
+  }
+
+  // consumers: warp (dmw, tw); thread words w = tw*32*P + lane + 32*p
+  const int dmw = warp / TW, tw = warp % TW;
+  const int dm = dm0 + dmw;
+  const int wbase = tw * 32 * P + lane;  // word index of p = 0 within the tile
+  BitCounter<P, L> cnt;
+  cnt.zero();
+  bool ok = true;
+  for (int k = 0; k < nslab; ++k) {
+    const int s = k % STAGES;
+    if (!mbar_wait(&full[s], (k / STAGES) & 1, a.status)) { ok = false; break; }
+    const int nc = min(SLAB, a.nchans - k * SLAB);
+    const uint32_t* sd = sdata + (int64_t)s * SLAB * NB * a.slot_w;
+    const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
+    const int32_t* bs = sbase + s * SLAB;
+    uint32_t c64[4][P];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {        // 16 channels
+      uint32_t cm[4][P];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {      // 4 channels
+        uint32_t x[NB][4][P];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int j = 16 * m + 4 * i + q;
+          const bool live = j < nc;
+          const int o = live ? (dl[j] - bs[j]) : 0;
+          const int wo = o >> 5, sh = o & 31;
+#pragma unroll
+          for (int b = 0; b < NB; ++b) {
+            const uint32_t* row = sd + (j * NB + b) * a.slot_w + wo + wbase;
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+              const uint32_t lo = live ? row[32 * p] : 0u;
+              const uint32_t hi = live ? row[32 * p + 1] : 0u;
+              x[b][q][p] = __funnelshift_r(lo, hi, sh);
+            }
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          if constexpr (NB == 2) {
+            const uint32_t lo[4] = {x[0][0][p], x[0][1][p], x[0][2][p], x[0][3][p]};
+            const uint32_t hi[4] = {x[NB - 1][0][p], x[NB - 1][1][p], x[NB - 1][2][p], x[NB - 1][3][p]};
+            cnt.quad2(p, lo, hi, cm[i][p]);   // weight 16
+          } else {
+            const uint32_t v[4] = {x[0][0][p], x[0][1][p], x[0][2][p], x[0][3][p]};
+            cnt.quad1(p, v, cm[i][p]);        // weight 4
+          }
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const uint32_t w4[4] = {cm[0][p], cm[1][p], cm[2][p], cm[3][p]};
+        if constexpr (NB == 2) cnt.fold4(p, 4, w4, c64[m][p]);   // -> weight 64
+        else cnt.fold4(p, 2, w4, c64[m][p]);                      // -> weight 16
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const uint32_t w4[4] = {c64[0][p], c64[1][p], c64[2][p], c64[3][p]};
+      uint32_t top;
+      if constexpr (NB == 2) {
+        cnt.fold4(p, 6, w4, top);  // weight 256
+        cnt.ripple(p, 8, top);
+      } else {
+        cnt.fold4(p, 4, w4, top);  // weight 64
+        cnt.ripple(p, 6, top);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  if (!ok || dm >= a.ndm) return;
+  // outputs: word p covers samples t0 + 32*(wbase + 32*p) + i
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const int64_t tb = t0 + 32LL * (wbase + 32 * p);
+    if (a.out_kind == SPP_OUT_I32) {
+      int32_t* out = static_cast<int32_t*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
+      if (tb + 32 <= a.nvalid && ((reinterpret_cast<uintptr_t>(out + tb) & 15) == 0)) {
+#pragma unroll
+        for (int i = 0; i < 32; i += 4) {
+          int4 v;
+          v.x = (int)cnt.count(p, i);
+          v.y = (int)cnt.count(p, i + 1);
+          v.z = (int)cnt.count(p, i + 2);
+          v.w = (int)cnt.count(p, i + 3);
+          *reinterpret_cast<int4*>(out + tb + i) = v;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i)
+          if (tb + i < a.nvalid) out[tb + i] = (int32_t)cnt.count(p, i);
+      }
+    } else if (a.out_kind == SPP_OUT_U16) {
+      uint16_t* out = static_cast<uint16_t*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (tb + i < a.nvalid) out[tb + i] = (uint16_t)min(cnt.count(p, i), 65535u);
+    } else {
+      float* out = static_cast<float*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
+#pragma unroll
+      for (int i = 0; i < 32; ++i)
+        if (tb + i < a.nvalid) out[tb + i] = (float)cnt.count(p, i);
+    }
+  }
+}
+
+// Corner turn into bit-plane rows (row c*NB + b: bit b of channel c, 32
+// samples per word).  CTA = 64 channels x 16 words (512 raw rows).
+template <int NB>
+__global__ void __launch_bounds__(256)
+k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t nsamps,
+                     int bitorder, int64_t halo, uint32_t* __restrict__ planar,
+                     int64_t pitch_w) {
+  constexpr int RT = kCtWords * 32;
+  constexpr int SB = kCtChans * NB / 8;
+  constexpr int SBP = SB + 4;
+  __shared__ __align__(16) uint8_t s_raw[RT * SBP];
+  __shared__ uint32_t s_out[kCtChans * NB][kCtWords + 1];
+  const int64_t c0 = (int64_t)blockIdx.x * kCtChans;
+  const int nc = (int)((nchans - c0) < kCtChans ? (nchans - c0) : kCtChans);
+  const int seg = (nc * NB + 7) / 8;
+  const int64_t rowbytes = nchans * NB / 8;
+  const int64_t segstart = c0 * NB / 8;
+  const bool vec = ((rowbytes & 3) == 0) && ((segstart & 3) == 0) && ((seg & 3) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(raw) & 3) == 0);
+  const int64_t ntw = (pitch_w + kCtWords - 1) / kCtWords;
+  for (int64_t by = blockIdx.y; by < ntw; by += gridDim.y) {
+    const int64_t w0 = by * kCtWords;
+    if (vec) {
+      const int nw = seg >> 2;
+      for (int idx = threadIdx.x; idx < RT * nw; idx += blockDim.x) {
+        const int r = idx / nw, k = idx - r * nw;
+        const int64_t row = wrap_row(w0 * 32 + r - halo, nsamps);
+        uint32_t v = 0;
+        if (row >= 0) v = __ldg(reinterpret_cast<const uint32_t*>(raw + row * rowbytes + segstart) + k);
+        *reinterpret_cast<uint32_t*>(s_raw + r * SBP + 4 * k) = v;
+      }
+    } else {
+      for (int idx = threadIdx.x; idx < RT * seg; idx += blockDim.x) {
+        const int r = idx / seg, k = idx - r * seg;
+        const int64_t row = wrap_row(w0 * 32 + r - halo, nsamps);
+        s_raw[r * SBP + k] = (row >= 0) ? __ldg(raw + row * rowbytes + segstart + k) : 0;
+      }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kCtChans * kCtWords; idx += blockDim.x) {
+      const int c = idx % kCtChans, w = idx / kCtChans;
+      uint32_t v[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) v[b] = 0;
+      if (c < nc) {
+        const int byte = (c * NB) / 8;
+#pragma unroll 8
+        for (int j = 0; j < 32; ++j) {
+          const uint32_t f = field_of<NB>(s_raw[(w * 32 + j) * SBP + byte], c, bitorder);
+#pragma unroll
+          for (int b = 0; b < NB; ++b) v[b] |= ((f >> b) & 1u) << j;
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b) s_out[c * NB + b][w] = v[b];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kCtChans * NB * kCtWords; idx += blockDim.x) {
+      const int w = idx % kCtWords, rr = idx / kCtWords;
+      if (rr < nc * NB && w0 + w < pitch_w) planar[(c0 * NB + rr) * pitch_w + w0 + w] = s_out[rr][w];
+    }
+    __syncthreads();
+  }
+}
 }  // namespace spp

@@ -493,7 +493,7 @@ int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n, int64_
   if (rc) return rc;
   const int64_t smem = (int64_t)(kSnrChunk + cfg.wmax + 1) * 8;
   if (smem > 48 * 1024) {
-    rc = cuda_status(cudaFuncSetAttribute(k_snr_chunk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "snr smem");
+    rc = set_smem_attr(reinterpret_cast<const void*>(k_snr_chunk), smem);
     if (rc) return rc;
   }
   dim3 grid((unsigned)nck, (unsigned)(nrows * nfactors));

@@ -12,7 +12,7 @@ DEFAULT_WIDTHS = (1, 2, 4, 8, 16, 32, 64, 128, 256)
 
 
 def boxcar_snr(rows: torch.Tensor, widths=DEFAULT_WIDTHS, factors=(1,), n: int | None = None,
-               stream: torch.cuda.Stream | None = None, with_index: bool = True):
+               stream: torch.cuda.Stream | None = None, with_index: bool = True, out=None):
     """S/N peak per (row, downsample factor, width) of a (nrows, >= n) CUDA tensor
     (float32 or int32): ``max_t (sum_{k<w} y[t+k] - w*mean(y)) / (std(y)*sqrt(w))``
     with ``y = downsample_mean(row, f)``.  Returns (snr float32, index int32)."""
@@ -25,8 +25,11 @@ def boxcar_snr(rows: torch.Tensor, widths=DEFAULT_WIDTHS, factors=(1,), n: int |
     n = rows.shape[1] if n is None else n
     fac = np.ascontiguousarray(factors, dtype=np.int32)
     wid = np.ascontiguousarray(widths, dtype=np.int32)
-    snr = torch.empty((nrows, fac.size, wid.size), dtype=torch.float32, device=rows.device)
-    idx = torch.empty_like(snr, dtype=torch.int32) if with_index else None
+    snr, idx = out if out is not None else (None, None)
+    if snr is None:
+        snr = torch.empty((nrows, fac.size, wid.size), dtype=torch.float32, device=rows.device)
+    if idx is None and with_index:
+        idx = torch.empty_like(snr, dtype=torch.int32)
     lib = _lib.load()
     need = lib.spp_boxcar_snr_workspace_bytes(nrows, n, fac.size, wid.size)
     ws = workspace(need, rows.device, stream)
