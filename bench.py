@@ -313,6 +313,133 @@ def run_gpu(args, rank, world, local):
     plan.close()
 
 
+def _line(**kw):
+    print(json.dumps(kw), flush=True)
+
+
+def run_c3(args, rank, world, local):
+    """Config 3: 64 beams of uneven length, two-stage subband search (32
+    subbands, 512 trials 0-1000), downsample 1/2/4, boxcar widths 1..256 ->
+    S/N peaks; each batch of beams is one CUDA graph of persistent launches.
+    Also times the plain per-call path (one brute-force dedispersion + S/N per
+    beam and DM) on a subset."""
+    import torch
+
+    from sigpyproc3_b200 import Header, multi, synth
+    from sigpyproc3_b200.dedisp import dedisperse_block
+    from sigpyproc3_b200.search import boxcar_snr
+    from sigpyproc3_b200.subband import SubbandPlan, SubbandSearch
+
+    g = synth.C3
+    h = Header(nchans=g.nchans, fch1=g.fch1, foff=g.foff, tsamp=g.tsamp, nbits=8)
+    plan = SubbandPlan(h, synth.dm_grid(500.0, 512), nsub=32, group=16)
+    rng = np.random.default_rng(3)
+    nbeams = args.beams
+    lens = rng.integers(1 << 18, (1 << 21) + 1, size=nbeams)
+    lo, hi = multi.shard_range(nbeams, rank, world)
+    th = synth.gauss_u8_thresholds(96.0, 12.0)
+    factors, widths = (1, 2, 4), tuple(1 << k for k in range(9))
+    batch = args.batch
+    # autotune the two stages on the first batch
+    tune_lens = lens[lo:lo + batch]
+    best, best_ms = (0, 0), None
+    for v1, v2 in ((0, 0), (1, 0), (2, 0), (3, 0)):
+        srch = SubbandSearch(plan, tune_lens, factors=factors, widths=widths, variants=(v1, v2))
+        for b in srch.beams:
+            synth.gauss_u8_device(b.raw.numel(), 99, 96.0, 12.0, out=b.raw)
+        srch.run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        srch.run(snr=False)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if best_ms is None or ms < best_ms:
+            best, best_ms = (v1, v2), ms
+        del srch
+        torch.cuda.empty_cache()
+    v1 = best[0]
+    best_ms = None
+    for v2 in range(4):
+        srch = SubbandSearch(plan, tune_lens, factors=factors, widths=widths, variants=(v1, v2))
+        for b in srch.beams:
+            synth.gauss_u8_device(b.raw.numel(), 99, 96.0, 12.0, out=b.raw)
+        srch.run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        srch.run(snr=False)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if best_ms is None or ms < best_ms:
+            best, best_ms = (v1, v2), ms
+        del srch
+        torch.cuda.empty_cache()
+    total_ms, units = 0.0, 0
+    peaks = []
+    torch.cuda.synchronize()
+    _barrier(world)
+    for b0 in range(lo, hi, batch):
+        blens = lens[b0:min(hi, b0 + batch)]
+        srch = SubbandSearch(plan, blens, factors=factors, widths=widths, variants=best)
+        for i, b in enumerate(srch.beams):
+            synth.gauss_u8_device(b.raw.numel(), 3000 + b0 + i, 96.0, 12.0, out=b.raw)
+        srch.capture()
+        for _ in range(args.warmup):
+            srch.replay()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            srch.replay()
+        e1.record()
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1) / args.steps
+        units += sum(512 * b.nvalid for b in srch.beams)
+        peaks += [float(b.snr.max()) for b in srch.beams]
+        assert srch.status_ok()
+        del srch
+        torch.cuda.empty_cache()
+    ms_max = multi.max_over_ranks(total_ms)
+    units_all = multi.sum_over_ranks(units)
+    value = units_all / (ms_max / 1e3)
+    # plain per-call path on a subset: 2 beams x 16 DMs, brute force + S/N per call
+    nsub_beams, nsub_dms = 2, 16
+    dms = plan.dms[np.linspace(0, 511, nsub_dms).astype(int)]
+    t_plain, u_plain = 0.0, 0
+    for bi in range(nsub_beams):
+        n = int(lens[bi])
+        raw = synth.gauss_u8_device(n * g.nchans, 3000 + bi, 96.0, 12.0)
+        d_all = np.atleast_2d(h.get_dmdelays(dms)).astype(np.int32)
+        nv = n - int(np.abs(d_all).max())
+        tim = torch.empty(nv + 8, dtype=torch.float32, device="cuda")
+        for dmi in range(nsub_dms):  # warm
+            dedisperse_block(raw, d_all[dmi], g.nchans, n, tim)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for dmi in range(nsub_dms):
+            d = d_all[dmi]
+            nvi = dedisperse_block(raw, d, g.nchans, n, tim)
+            boxcar_snr(tim[:nvi].view(1, -1), widths=widths, factors=factors)
+            u_plain += nvi
+        torch.cuda.synchronize()
+        t_plain += time.perf_counter() - t0
+    plain = u_plain / t_plain
+    if rank == 0:
+        _line(metric="DM-trial x samples/s, config 3 (batched two-stage subband search + S/N)",
+              value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+              ms_per_step=ms_max, higher_is_better=True, scaling="weak", vs_baseline=None,
+              dtype="u8->uint16->int32 (+f32 S/N)", data="synthetic (device generator, seeded)",
+              config={"workload": f"config 3: {nbeams} beams nsamps U[2^18,2^21], 1024 ch 8-bit, "
+                      "32 subbands x 16-trial groups, 512 trials 0-1000, downsample 1/2/4, "
+                      "widths 1..256", "batch_beams": batch, "variants": list(best),
+                      "beams_total_samples": int(lens.sum())},
+              plain_per_call={"value": plain, "unit": UNIT, "path": "dedisperse_block + boxcar_snr "
+                              "per (beam, DM), brute force over 1024 channels",
+                              "sample": f"{nsub_beams} beams x {nsub_dms} DMs"},
+              served_over_plain=value / plain, max_snr=max(peaks) if peaks else None,
+              gpu_launches=None)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -322,6 +449,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="fix the kernel variant")
+    ap.add_argument("--workload", choices=["c2", "c3", "c4", "c1", "c5"], default="c2")
+    ap.add_argument("--beams", type=int, default=64, help="config 3: number of beams")
+    ap.add_argument("--batch", type=int, default=4, help="config 3: beams per graph")
+    ap.add_argument("--chunks", type=int, default=128, help="config 4: chunks served")
+    ap.add_argument("--budget-gb", type=float, default=48.0, help="config 4: HBM budget")
     ap.add_argument("--ndm", type=int, default=None, help="profiling only: fewer DM trials")
     ap.add_argument("--nsamps", type=int, default=None, help="profiling only: fewer samples")
     args = ap.parse_args()
@@ -332,7 +464,14 @@ def main():
         return
     rank, world, local = _dist_init()
     try:
-        run_gpu(args, rank, world, local)
+        if args.workload == "c3":
+            run_c3(args, rank, world, local)
+        elif args.workload == "c2":
+            run_gpu(args, rank, world, local)
+        else:
+            from sigpyproc3_b200 import workloads
+
+            workloads.run(args.workload, args, rank, world, local, _line)
     finally:
         if world > 1:
             import torch.distributed as dist

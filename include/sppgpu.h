@@ -129,6 +129,15 @@ int spp_dmt_plan_timing_read(spp_dmt_plan* plan, double* ms_corner_turn,
 int spp_dmt_execute(const spp_dmt_plan* plan, const void* in, int64_t nsamps,
                     void* out, int64_t out_stride, int64_t out_start,
                     void* workspace, int64_t workspace_bytes, void* stream);
+/* Float32 input with the zero-DM filter of kernels.remove_zerodm
+ * (core/kernels.py:465-505) fused into the load: every sample becomes
+ * f32((f64(x) - zdm[t]*f64(chanwts[c])) + f64(bpass[c])), zdm[t] = sum_c f64(x[t][c]),
+ * before the transform.  bpass/chanwts are device float arrays (nchans). */
+int64_t spp_dmt_plan_zero_dm_workspace_bytes(const spp_dmt_plan* plan, int64_t nsamps);
+int spp_dmt_execute_zero_dm(const spp_dmt_plan* plan, const float* in, int64_t nsamps,
+                            const float* bpass, const float* chanwts, void* out,
+                            int64_t out_stride, int64_t out_start, void* workspace,
+                            int64_t workspace_bytes, void* stream);
 /* Same transform end to end from HOST memory: `in_host` (pinned or pageable)
  * and `out_host` (ndm x out_stride elements).  Time is cut into blocks of
  * `block_nsamps` output samples; H2D, compute and D2H of successive blocks

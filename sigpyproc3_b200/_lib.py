@@ -58,6 +58,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_dmt_plan_timing": ([_p, _int], _int),
     "spp_dmt_plan_timing_read": ([_p, _p, _p, _p], _int),
     "spp_dmt_execute": ([_p, _p, _i64, _p, _i64, _i64, _p, _i64, _p], _int),
+    "spp_dmt_plan_zero_dm_workspace_bytes": ([_p, _i64], _i64),
+    "spp_dmt_execute_zero_dm": ([_p, _p, _i64, _p, _p, _p, _i64, _i64, _p, _i64, _p], _int),
     "spp_dmt_execute_host": ([_p, _p, _i64, _p, _i64, _i64, _p, _i64], _int),
     "spp_dmt_host_workspace_bytes": ([_p, _i64], _i64),
     "spp_bandpass": ([_p, _int, _int, _i64, _i64, _p, _p], _int),

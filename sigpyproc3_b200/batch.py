@@ -85,6 +85,8 @@ class WorkList:
         out_ptr + r * out_stride * out_elem."""
         dh = np.atleast_2d(delays_host).astype(np.int64) * sign
         ndm = dh.shape[0]
+        if delays_dev.dtype != torch.int32 or delays_dev.stride(-1) != 1:
+            raise ValueError("delays_dev must be int32 with unit stride along channels")
         dpitch = delays_dev.stride(0) if delays_dev.dim() == 2 else nchans
         T, DW = self.T, self.DW
         ntiles = max(1, -(-nvalid // T))

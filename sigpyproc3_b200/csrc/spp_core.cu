@@ -534,7 +534,8 @@ int64_t spp_dmt_plan_workspace_bytes(const spp_dmt_plan* p, int64_t nsamps) {
 
 static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* out,
                    int64_t out_stride, int64_t out_start, uint8_t* ws, int64_t ws_bytes,
-                   cudaStream_t st) {
+                   cudaStream_t st, const float* zd_bpass = nullptr,
+                   const float* zd_chanwts = nullptr, double* zd_rows = nullptr) {
   int slot;
   Geometry g = plan_geometry(p, nsamps, &slot);
   if (g.nvalid <= 0) return SPP_OK;
@@ -561,7 +562,15 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
     }
     cudaEventRecord(ev[0], st);
   }
-  int rc = launch_corner_turn(p->nbits, in, p->bitorder, p->nchans, nsamps, g, planar, st);
+  int rc = SPP_OK;
+  if (zd_rows) {
+    const unsigned blocks = (unsigned)ceil_div(nsamps, 8);
+    k_row_sum_f64<<<blocks, 256, 0, st>>>(static_cast<const float*>(in), p->nchans, nsamps, zd_rows);
+    rc = cuda_status(cudaGetLastError(), "zero-DM row sums");
+    if (rc) return rc;
+  }
+  rc = launch_corner_turn(p->nbits, in, p->bitorder, p->nchans, nsamps, g, planar, st, zd_rows,
+                          zd_chanwts, zd_bpass);
   if (rc) return rc;
   if (p->timing) cudaEventRecord(ev[1], st);
   DmtArgs a{};
@@ -628,6 +637,27 @@ int spp_dmt_execute(const spp_dmt_plan* p, const void* in, int64_t nsamps, void*
     return fail(SPP_ERR_ALIGN, "workspace must be 256-B aligned");
   return dmt_run(p, in, nsamps, out, out_stride, out_start, static_cast<uint8_t*>(workspace),
                  workspace_bytes, as_stream(stream));
+}
+
+int64_t spp_dmt_plan_zero_dm_workspace_bytes(const spp_dmt_plan* p, int64_t nsamps) {
+  if (!p) return -1;
+  return spp_dmt_plan_workspace_bytes(p, nsamps) + round_up(nsamps * 8, 256);
+}
+
+int spp_dmt_execute_zero_dm(const spp_dmt_plan* p, const float* in, int64_t nsamps,
+                            const float* bpass, const float* chanwts, void* out,
+                            int64_t out_stride, int64_t out_start, void* workspace,
+                            int64_t workspace_bytes, void* stream) {
+  if (!p || !in || !bpass || !chanwts || !out || !workspace) return fail(SPP_ERR_ARG, "null pointer");
+  if (p->nbits != 32) return fail(SPP_ERR_UNSUPPORTED, "zero-DM fusion needs float32 input");
+  if (nsamps <= 0 || nsamps > p->nsamps_max) return fail(SPP_ERR_SIZE, "nsamps out of range");
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return fail(SPP_ERR_ALIGN, "workspace must be 256-B aligned");
+  const int64_t need = spp_dmt_plan_zero_dm_workspace_bytes(p, nsamps);
+  if (workspace_bytes < need) return fail(SPP_ERR_SIZE, "workspace %lld < %lld", (long long)workspace_bytes, (long long)need);
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  double* rows = reinterpret_cast<double*>(ws + spp_dmt_plan_workspace_bytes(p, nsamps));
+  return dmt_run(p, in, nsamps, out, out_stride, out_start, ws, workspace_bytes, as_stream(stream),
+                 bpass, chanwts, rows);
 }
 
 // --- end-to-end from host buffers ------------------------------------------------

@@ -234,6 +234,25 @@ class DMTPlan:
             ws.numel(), stream_handle(stream, raw.device)))
         return out
 
+    def execute_zero_dm(self, raw: torch.Tensor, nsamps: int, bpass: torch.Tensor,
+                        chanwts: torch.Tensor, out: torch.Tensor | None = None, out_start: int = 0,
+                        stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+        """Float32 input with kernels.remove_zerodm fused into the load."""
+        raw = _as_raw(raw)
+        lib = _lib.load()
+        nv = self.nvalid(nsamps)
+        if out is None:
+            out = torch.empty((self.ndm, nv), dtype=self.out_dtype, device=raw.device)
+        stride = out.stride(0) if out.dim() == 2 else out.numel()
+        ws = workspace(int(lib.spp_dmt_plan_zero_dm_workspace_bytes(self._h, nsamps)), raw.device,
+                       stream)
+        bpass = bpass.contiguous()
+        chanwts = chanwts.to(torch.float32).contiguous()
+        _lib.check(lib.spp_dmt_execute_zero_dm(
+            self._h, raw.data_ptr(), nsamps, bpass.data_ptr(), chanwts.data_ptr(), out.data_ptr(),
+            stride, out_start, ws.data_ptr(), ws.numel(), stream_handle(stream, raw.device)))
+        return out
+
     def host_workspace_bytes(self, block_nsamps: int) -> int:
         return int(_lib.load().spp_dmt_host_workspace_bytes(self._h, block_nsamps))
 

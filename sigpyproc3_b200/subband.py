@@ -59,11 +59,12 @@ class SubbandPlan:
         rel = dn - dn[:, self.ref_chan[sub_of]]
         if rel.min() < 0:
             raise ValueError("subband reference channel is not the least-delayed channel")
-        self.rel = rel.astype(np.int32)                     # (ngroups, nchans)
+        self.rel = np.ascontiguousarray(rel, dtype=np.int32)            # (ngroups, nchans)
         d = np.atleast_2d(h.get_dmdelays(self.dms, ref_freq)).astype(np.int64)
-        self.dsub = d[:, self.ref_chan].astype(np.int32)     # (ndm, nsub)
+        self.dsub = np.ascontiguousarray(d[:, self.ref_chan], dtype=np.int32)  # (ndm, nsub)
         g_of = np.arange(self.ndm) // group
-        self.eff = (self.dsub[:, sub_of].astype(np.int64) + rel[g_of]).astype(np.int32)
+        self.eff = np.ascontiguousarray(self.dsub[:, sub_of].astype(np.int64) + rel[g_of],
+                                        dtype=np.int32)
         self.max_rel = int(self.rel.max())
         self.max_eff = int(self.eff.max())
 
