@@ -410,8 +410,7 @@ def run_c3(args, rank, world, local):
         n = int(lens[bi])
         raw = synth.gauss_u8_device(n * g.nchans, 3000 + bi, 96.0, 12.0)
         d_all = np.atleast_2d(h.get_dmdelays(dms)).astype(np.int32)
-        nv = n - int(np.abs(d_all).max())
-        tim = torch.empty(nv + 8, dtype=torch.float32, device="cuda")
+        tim = torch.empty(n, dtype=torch.float32, device="cuda")
         for dmi in range(nsub_dms):  # warm
             dedisperse_block(raw, d_all[dmi], g.nchans, n, tim)
         torch.cuda.synchronize()

@@ -95,6 +95,26 @@ int spp_dedisperse(const void* in, int nbits, int bitorder, int64_t nchans,
                    int64_t out_start, int acc, void* workspace,
                    int64_t workspace_bytes, void* stream);
 
+/* Same computation as spp_dedisperse, but allocating nothing and taking no
+ * workspace.  No counterpart in the reference.  It serves callers that must not
+ * allocate device memory while running (a real-time pipeline that reserves its
+ * memory at start-up and treats a later cudaMalloc -- which may synchronise the
+ * device or fail under memory pressure -- as an error, or a host framework whose
+ * allocator owns device memory and hands out only input and output buffers).
+ * Its scratch is a fixed array of spp_dedisperse_noalloc_max_bytes() (32 MiB)
+ * compiled into the library, which every GPU that loads the library holds until
+ * the process exits; blocks whose scratch would exceed it are rejected with
+ * SPP_ERR_SIZE.  The first call on each device looks the array up with
+ * cudaGetSymbolAddress, so make that first call before any stream capture.
+ * All calls share the one array and leave the last call's data in it: calls
+ * that can overlap on the GPU (different streams, or several host threads)
+ * race with each other and must be serialised by the caller. */
+int64_t spp_dedisperse_noalloc_max_bytes(void);
+int spp_dedisperse_noalloc(const void* in, int nbits, int bitorder, int64_t nchans,
+                           int64_t nsamps, const int32_t* delays, int32_t delay_min,
+                           int32_t delay_max, float* out, int64_t out_len,
+                           int64_t out_start, int acc, void* stream);
+
 /* ---- R3: DM-trial batch (DM-time transform) -----------------------------------
  * Replaces FilterbankBlock.dmt_transform (block.py:309-343) / kernels.dmt_block
  * (core/kernels.py:1155-1168).  A plan owns the ndm x nchans delay table on the

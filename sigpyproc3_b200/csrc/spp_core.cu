@@ -106,7 +106,7 @@ static const std::vector<Variant>& variants() {
       SPP_INT_VARIANTS(2),
       SPP_INT_VARIANTS(4),
       SPP_INT_VARIANTS(8),
-      mk<8, 4, 1, 8, 64, 3, 0>(1),
+      mk<8, 4, 1, 4, 16, 3, 0>(1),
       // float32 input, compensated fp32
       mk<32, 8, 8, 1, 32, 2, SPP_ACC_KAHAN32>(0),
       mk<32, 4, 8, 2, 32, 2, SPP_ACC_KAHAN32>(0),
@@ -234,6 +234,7 @@ static int pick_single_variant(int nb, int acc, int64_t nvalid) {
   for (int i = 0; i < (int)vs.size(); ++i) {
     const Variant& v = vs[i];
     if (!v.single || v.nb != nb || (nb == 32 && v.acc != acc)) continue;
+    if (smem_bytes(v, slot_words(v, 0)) > kMaxSmem) continue;
     const int64_t T = tile_T(v);
     if (ceil_div(nvalid, T) >= 296 && (best_big < 0 || T > tile_T(vs[best_big]))) best_big = i;
     if (best_small < 0 || T < tile_T(vs[best_small])) best_small = i;
@@ -349,6 +350,106 @@ int spp_dedisperse(const void* in, int nbits, int bitorder, int64_t nchans, int6
     return fail(SPP_ERR_ALIGN, "workspace must be 256-B aligned");
   cudaStream_t st = as_stream(stream);
   uint8_t* ws = static_cast<uint8_t*>(workspace);
+  void* planar = ws + kStatusBytes;
+  rc = launch_corner_turn(nbits, in, bitorder, nchans, nsamps, g, planar, st);
+  if (rc) return rc;
+  DmtArgs a{};
+  a.planar = planar;
+  a.pitch_w = g.pitch_w;
+  a.halo = g.halo;
+  a.nchans = (int32_t)nchans;
+  a.delays = delays;
+  a.dpitch = nchans;
+  a.ndm = 1;
+  a.sign = 1;
+  a.dlo = delay_min;
+  a.dhi = delay_max;
+  a.span_max = 0;
+  a.slot_w = slot;
+  a.out = out;
+  a.out_kind = SPP_OUT_F32;
+  a.out_stride = 0;
+  a.out_start = out_start;
+  a.nvalid = g.nvalid;
+  a.status = reinterpret_cast<uint32_t*>(ws);
+  return launch_dmt(*v, a, g.ntiles_t, 1, st);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Single-DM dedispersion without allocation.
+//
+// For callers that must not allocate device memory once they are running --
+// e.g. a real-time search pipeline that reserves its device memory at
+// start-up and treats any later cudaMalloc (which can synchronise the device
+// and can fail under memory pressure) as an error, or a host framework whose
+// own allocator owns the device memory and hands out only input and output
+// buffers.  The scratch that spp_dedisperse takes as `workspace` lives here
+// in a fixed device array instead.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kNoAllocScratchBytes = 32ll << 20;  // 32 MiB per device
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array for the current device, looked up
+// once per device (the symbol name is only a host-side handle).
+int noalloc_scratch(void** out) {
+  int dev = 0;
+  int rc = cuda_status(cudaGetDevice(&dev), "cudaGetDevice");
+  if (rc) return rc;
+  if (dev < 0 || dev >= kMaxDevices) return fail(SPP_ERR_UNSUPPORTED, "device index %d", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    rc = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+    if (rc) return rc;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return SPP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int64_t spp_dedisperse_noalloc_max_bytes(void) { return kNoAllocScratchBytes; }
+
+int spp_dedisperse_noalloc(const void* in, int nbits, int bitorder, int64_t nchans,
+                           int64_t nsamps, const int32_t* delays, int32_t delay_min,
+                           int32_t delay_max, float* out, int64_t out_len, int64_t out_start,
+                           int acc, void* stream) {
+  if (!in || !delays || !out) return fail(SPP_ERR_ARG, "spp_dedisperse_noalloc: null pointer");
+  if (acc != SPP_ACC_F64 && acc != SPP_ACC_KAHAN32) return fail(SPP_ERR_ARG, "bad acc %d", acc);
+  const Variant* v;
+  Geometry g;
+  int slot;
+  int rc = single_setup(nbits, nchans, nsamps, delay_min, delay_max, acc, &v, &g, &slot);
+  if (rc) return rc;
+  if (g.nvalid <= 0) return SPP_OK;
+  if (out_start < 0 || out_start + g.nvalid > out_len)
+    return fail(SPP_ERR_SIZE, "output too small: out_start %lld + %lld samples > out_len %lld",
+                (long long)out_start, (long long)g.nvalid, (long long)out_len);
+  const int64_t need = kStatusBytes + g.bytes;
+  if (need > kNoAllocScratchBytes)
+    return fail(SPP_ERR_SIZE,
+                "block needs %lld B of scratch, above the fixed %lld B of the no-allocation "
+                "entry point: use spp_dedisperse with a workspace, or smaller blocks",
+                (long long)need, (long long)kNoAllocScratchBytes);
+  void* base = nullptr;
+  rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  uint8_t* ws = static_cast<uint8_t*>(base);
+  // the status block must start at zero; the planar rows are fully rewritten
+  rc = cuda_status(cudaMemsetAsync(ws, 0, kStatusBytes, st), "status clear");
+  if (rc) return rc;
   void* planar = ws + kStatusBytes;
   rc = launch_corner_turn(nbits, in, bitorder, nchans, nsamps, g, planar, st);
   if (rc) return rc;

@@ -370,9 +370,12 @@ k_dmt(const DmtArgs a) {
   }
 
   // ---------------- consumer warps ----------------
+  // Thread (warp (dmw, tw), lane) owns words wbase + lane + 32*r, r < R, of the
+  // tile (interleaved across the warp so every shared-memory load of a warp
+  // touches 32 consecutive words: no bank conflicts).
   const int dmw = warp / TW, tw = warp % TW;
   const int dm = dm0 + dmw;
-  const int tloc = tw * (32 * R * SPW) + lane * (R * SPW);
+  const int wbase = tw * 32 * R + lane;
   bool ok = true;
 
   if constexpr (NB == 32) {
@@ -390,10 +393,10 @@ k_dmt(const DmtArgs a) {
       const int32_t* bs = sbase + s * SLAB;
 #pragma unroll 4
       for (int j = 0; j < nc; ++j) {
-        const float* row = sd + j * a.slot_w + (tloc + dl[j] - bs[j]);
+        const float* row = sd + j * a.slot_w + (wbase + dl[j] - bs[j]);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const float x = row[r];
+          const float x = row[32 * r];
           if (ACC == SPP_ACC_F64) {
             d_acc[r] += (double)x;
           } else {
@@ -411,7 +414,7 @@ k_dmt(const DmtArgs a) {
     float* out = static_cast<float*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int64_t t = t0 + tloc + r;
+      const int64_t t = t0 + wbase + 32 * r;
       if (t < a.nvalid)
         out[t] = (ACC == SPP_ACC_F64) ? (float)d_acc[r] : __fsub_rn(s_acc[r], c_acc[r]);
     }
@@ -433,14 +436,12 @@ k_dmt(const DmtArgs a) {
         const int je = min(nc, jb + F8);
 #pragma unroll 4
         for (int j = jb; j < je; ++j) {
-          const int o = tloc + dl[j] - bs[j];
-          const uint32_t* row = sd + j * a.slot_w + (o >> P::kLogSpw);
+          const int o = dl[j] - bs[j];  // sample offset of the tile start in the slot
+          const uint32_t* row = sd + j * a.slot_w + (o >> P::kLogSpw) + wbase;
           const int sh = (o & (SPW - 1)) * NB;
-          uint32_t w[R + 1];
 #pragma unroll
-          for (int r = 0; r <= R; ++r) w[r] = row[r];
-#pragma unroll
-          for (int r = 0; r < R; ++r) acc.add(__funnelshift_r(w[r], w[r + 1], sh), r);
+          for (int r = 0; r < R; ++r)
+            acc.add(__funnelshift_r(row[32 * r], row[32 * r + 1], sh), r);
         }
         acc.flush8();
       }
@@ -450,14 +451,13 @@ k_dmt(const DmtArgs a) {
     }
     acc.flush16();
     if (!ok || dm >= a.ndm) return;
-    const int64_t tb = t0 + tloc;
     if (a.out_kind == SPP_OUT_U16) {
       uint16_t* out = static_cast<uint16_t*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
 #pragma unroll
       for (int r = 0; r < R; ++r)
 #pragma unroll
         for (int j = 0; j < SPW; ++j) {
-          const int64_t t = tb + r * SPW + j;
+          const int64_t t = t0 + (int64_t)(wbase + 32 * r) * SPW + j;
           if (t < a.nvalid) out[t] = (uint16_t)min(acc.S[r][j], 65535u);
         }
     } else if (a.out_kind == SPP_OUT_I32) {
@@ -466,7 +466,7 @@ k_dmt(const DmtArgs a) {
       for (int r = 0; r < R; ++r)
 #pragma unroll
         for (int j = 0; j < SPW; ++j) {
-          const int64_t t = tb + r * SPW + j;
+          const int64_t t = t0 + (int64_t)(wbase + 32 * r) * SPW + j;
           if (t < a.nvalid) out[t] = (int32_t)acc.S[r][j];
         }
     } else {
@@ -475,13 +475,12 @@ k_dmt(const DmtArgs a) {
       for (int r = 0; r < R; ++r)
 #pragma unroll
         for (int j = 0; j < SPW; ++j) {
-          const int64_t t = tb + r * SPW + j;
+          const int64_t t = t0 + (int64_t)(wbase + 32 * r) * SPW + j;
           if (t < a.nvalid) out[t] = (float)acc.S[r][j];
         }
     }
   }
 }
-
 
 // ----------------------------------------------------------------------------
 // Persistent work-list DM-time kernel.  Each work item is one DM tile (up to
@@ -524,14 +523,14 @@ struct WlArgs {
 
 template <int NB, int R, int SPW>
 __device__ __forceinline__ void store_int_outputs(const IntAcc<NB, R>& acc, const DmtItem& it,
-                                                  int row, int64_t tb) {
+                                                  int row, int64_t t0, int wbase) {
   if (it.out_kind == SPP_OUT_U16) {
     uint16_t* out = static_cast<uint16_t*>(it.out) + (int64_t)row * it.out_stride + it.out_start;
 #pragma unroll
     for (int r = 0; r < R; ++r)
 #pragma unroll
       for (int j = 0; j < SPW; ++j) {
-        const int64_t t = tb + r * SPW + j;
+        const int64_t t = t0 + (int64_t)(wbase + 32 * r) * SPW + j;
         if (t < it.nvalid) out[t] = (uint16_t)min(acc.S[r][j], 65535u);
       }
   } else if (it.out_kind == SPP_OUT_I32) {
@@ -540,7 +539,7 @@ __device__ __forceinline__ void store_int_outputs(const IntAcc<NB, R>& acc, cons
     for (int r = 0; r < R; ++r)
 #pragma unroll
       for (int j = 0; j < SPW; ++j) {
-        const int64_t t = tb + r * SPW + j;
+        const int64_t t = t0 + (int64_t)(wbase + 32 * r) * SPW + j;
         if (t < it.nvalid) out[t] = (int32_t)acc.S[r][j];
       }
   } else {
@@ -549,7 +548,7 @@ __device__ __forceinline__ void store_int_outputs(const IntAcc<NB, R>& acc, cons
     for (int r = 0; r < R; ++r)
 #pragma unroll
       for (int j = 0; j < SPW; ++j) {
-        const int64_t t = tb + r * SPW + j;
+        const int64_t t = t0 + (int64_t)(wbase + 32 * r) * SPW + j;
         if (t < it.nvalid) out[t] = (float)acc.S[r][j];
       }
   }
@@ -664,8 +663,9 @@ k_dmt_wl(const WlArgs w) {
   }
 
   // ---------------- consumer warps ----------------
+  // words wbase + lane + 32*r of the tile (interleaved: conflict-free loads)
   const int dmw = warp / TW, tw = warp % TW;
-  const int tloc = tw * (32 * R * SPW) + lane * (R * SPW);
+  const int wbase = tw * 32 * R + lane;
   uint32_t gk = 0;
   if constexpr (NB == 32) {
     float s_acc[R], c_acc[R];
@@ -688,10 +688,10 @@ k_dmt_wl(const WlArgs w) {
       const int32_t* bs = sbase + s * SLAB;
 #pragma unroll 4
       for (int j = 0; j < nc; ++j) {
-        const float* row = sd + j * w.slot_w + (tloc + dl[j] - bs[j]);
+        const float* row = sd + j * w.slot_w + (wbase + dl[j] - bs[j]);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const float x = row[r];
+          const float x = row[32 * r];
           if (ACC == SPP_ACC_F64) {
             d_acc[r] += (double)x;
           } else {
@@ -708,7 +708,7 @@ k_dmt_wl(const WlArgs w) {
         float* out = static_cast<float*>(it.out) + (int64_t)dmw * it.out_stride + it.out_start;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const int64_t t = it.t0 + tloc + r;
+          const int64_t t = it.t0 + wbase + 32 * r;
           if (t < it.nvalid)
             out[t] = (ACC == SPP_ACC_F64) ? (float)d_acc[r] : __fsub_rn(s_acc[r], c_acc[r]);
         }
@@ -738,14 +738,12 @@ k_dmt_wl(const WlArgs w) {
         const int je = min(nc, jb + F8);
 #pragma unroll 4
         for (int j = jb; j < je; ++j) {
-          const int o = tloc + dl[j] - bs[j];
-          const uint32_t* row = sd + j * w.slot_w + (o >> P::kLogSpw);
+          const int o = dl[j] - bs[j];
+          const uint32_t* row = sd + j * w.slot_w + (o >> P::kLogSpw) + wbase;
           const int sh = (o & (SPW - 1)) * NB;
-          uint32_t wv[R + 1];
 #pragma unroll
-          for (int r = 0; r <= R; ++r) wv[r] = row[r];
-#pragma unroll
-          for (int r = 0; r < R; ++r) acc.add(__funnelshift_r(wv[r], wv[r + 1], sh), r);
+          for (int r = 0; r < R; ++r)
+            acc.add(__funnelshift_r(row[32 * r], row[32 * r + 1], sh), r);
         }
         acc.flush8();
       }
@@ -754,7 +752,7 @@ k_dmt_wl(const WlArgs w) {
       if (((k + 1) % K16) == 0) acc.flush16();
       if (k == nslab - 1) {
         acc.flush16();
-        if (dmw < it.nrows) store_int_outputs<NB, R, SPW>(acc, it, dmw, it.t0 + tloc);
+        if (dmw < it.nrows) store_int_outputs<NB, R, SPW>(acc, it, dmw, it.t0, wbase);
       }
     }
   }

@@ -3,10 +3,11 @@ from many beams on one GPU.
 
 Each beam has its own geometry (nchans, nbits, band), DM trials and delay
 table, resident in HBM for the life of the beam ("DM plan" state), and a
-device-resident overlap tail: the last ``maxd`` raw rows of its stream.  A
-chunk of ``n`` new samples is processed as [tail | chunk] (n + maxd rows),
-which yields exactly ``n`` new DM-time samples per trial (the first chunk of
-a beam, with no tail yet, yields n - maxd) -- the same outputs as running
+device-resident overlap tail: the last ``maxd`` raw rows of its stream
+(right-aligned; ``hist`` of them are real once the stream is shorter than
+``maxd``).  A chunk of ``n`` new samples is processed as [tail | chunk] from
+the first real row, which yields ``hist + n - maxd`` new DM-time samples per
+trial (``n`` once the tail is full) -- exactly the outputs of running
 Filterbank.dedisperse over the concatenated stream.
 
 The server loop admits arrived chunks in FIFO order while their working set
@@ -70,7 +71,7 @@ class BeamState:
         self.ndm = self.delays.shape[0]
         self.delays_dev = torch.from_numpy(self.delays).to(device)
         self.tail = torch.zeros(max(self.maxd, 1) * self.row_bytes, dtype=torch.uint8, device=device)
-        self.has_tail = False
+        self.hist = 0  # real stream rows held (right-aligned) in the tail, <= maxd
         self.next_seq = 0
         self.bitorder = _lib.BITORDER_LITTLE if h.nbits == 1 else _lib.BITORDER_BIG
 
@@ -159,15 +160,10 @@ class Server:
                 raw[head:].copy_(src.view(-1)[: c.nsamps * st.row_bytes], non_blocking=True)
                 if st.maxd:
                     st.tail.copy_(raw[rows * st.row_bytes - head:], non_blocking=True)
-            first = not st.has_tail
-            st.has_tail = True
-            if first:
-                # no tail yet: outputs start at the chunk's maxd-th sample
-                c.nvalid = c.nsamps - st.maxd
-                start_row = st.maxd
-            else:
-                c.nvalid = c.nsamps
-                start_row = 0
+            # real rows start after the part of the tail not yet filled by the stream
+            start_row = st.maxd - st.hist
+            c.nvalid = st.hist + c.nsamps - st.maxd
+            st.hist = min(st.maxd, st.hist + c.nsamps)
             groups.setdefault(st.nbits, []).append((c, st, raw, start_row))
             total += self.chunk_bytes(c)
         stream.wait_stream(cs)
@@ -280,19 +276,22 @@ def plain_process(beams: dict[int, BeamState] | None, chunk: Chunk, st: BeamStat
     rows = chunk.nsamps + st.maxd
     raw = torch.empty(rows * st.row_bytes, dtype=torch.uint8, device=dev)
     head = st.maxd * st.row_bytes
-    first = not st.has_tail
     if st.maxd:
         raw[:head].copy_(st.tail)
     src = chunk.data if torch.is_tensor(chunk.data) else torch.from_numpy(chunk.data)
     raw[head:].copy_(src.view(-1)[: chunk.nsamps * st.row_bytes])
     if st.maxd:
         st.tail.copy_(raw[rows * st.row_bytes - head:])
-    st.has_tail = True
-    start_row = st.maxd if first else 0
+    start_row = st.maxd - st.hist
+    chunk.nvalid = st.hist + chunk.nsamps - st.maxd
+    st.hist = min(st.maxd, st.hist + chunk.nsamps)
+    if chunk.nvalid <= 0:
+        chunk.nvalid = 0
+        return chunk
     plan = DMTPlan(st.delays, st.nchans, rows, nbits=st.nbits,
                    bitorder="little" if st.nbits == 1 else "big", out_dtype=torch.int32)
     dmt = plan.execute(raw[start_row * st.row_bytes:], rows - start_row)
-    chunk.nvalid = dmt.shape[1]
+    assert dmt.shape[1] == chunk.nvalid
     if chunk.nvalid > 0:
         snr, _ = boxcar_snr(dmt, widths=widths, factors=(1,), with_index=False)
         chunk.snr = snr.cpu().numpy().reshape(-1, len(widths))

@@ -148,9 +148,25 @@ def run_c5(args, rank, world, local, emit) -> None:
     x = synth.gauss_f32_device(nsamps * g.nchans, 5)
     h = Header(nchans=g.nchans, fch1=g.fch1, foff=g.foff, tsamp=g.tsamp, nbits=32,
                nsamples=nsamps)
-    plan = DMTPlan(d, g.nchans, nsamps, nbits=32, acc=_lib.ACC_KAHAN32)
-    nv = plan.nvalid(nsamps)
+    nv = nsamps - int(d.max())
     out = torch.empty((ndm, nv), dtype=torch.float32, device="cuda")
+    # pick the accumulator and tile shape by timing one transform of each
+    tune = []
+    for acc in (_lib.ACC_KAHAN32, _lib.ACC_F64):
+        p = DMTPlan(d, g.nchans, nsamps, nbits=32, acc=acc)
+        for v in range(p.num_variants):
+            p.set_variant(v)
+            p.execute(x, nsamps, out)
+            e0, e1 = _events()
+            e0.record()
+            p.execute(x, nsamps, out)
+            e1.record()
+            e1.synchronize()
+            tune.append((e0.elapsed_time(e1), acc, v))
+        p.close()
+    best = min(tune)
+    plan = DMTPlan(d, g.nchans, nsamps, nbits=32, acc=best[1])
+    plan.set_variant(best[2])
     widths = tuple(1 << k for k in range(10))
     bp = torch.zeros(g.nchans, dtype=torch.float32, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
@@ -181,7 +197,9 @@ def run_c5(args, rank, world, local, emit) -> None:
              ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
              dtype="f32 (compensated fp32 sums)", data="synthetic N(0,1) on device (seed 5)",
              config={"workload": f"config 5: float32 {g.nchans} ch x {nsamps}, zero-DM, {ndm} "
-                     "trials 0-3000, boxcar widths 1..512", "tile": plan.describe()},
+                     "trials 0-3000, boxcar widths 1..512", "tile": plan.describe(),
+                     "accumulator": "fp64" if best[1] == _lib.ACC_F64 else "kahan fp32",
+                     "autotune_ms": [round(t[0], 2) for t in tune]},
              kernel_ms={"dmt": dmt_ms, "corner_turn_zero_dm": tk["ms_corner_turn"] / max(tk["n"], 1)},
              fp32_adds_per_s=adds / (dmt_ms / 1e3), max_snr=float(snr.max()))
     plan.close()

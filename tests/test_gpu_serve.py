@@ -112,3 +112,34 @@ def test_admission_respects_budget(torch_cuda):
         assert one.in_use <= one.budget
         assert all(len(b.chunks) == 1 for b in one.inflight)
     assert len(one.done) == 4
+
+
+def test_short_first_chunks(torch_cuda, orc):
+    """Chunks shorter than the max delay: outputs start once the stream covers it."""
+    torch = torch_cuda
+    from sigpyproc3_b200.serve import BeamState, Chunk, Server, plain_process
+
+    spec = _beams()[0]
+    st0 = BeamState(spec, torch.device("cuda", 0))
+    maxd = st0.maxd
+    lens = np.array([maxd // 3, maxd // 2, 4000, 100])
+    rng = np.random.default_rng(12)
+    vals = [rng.integers(0, 256, size=n * spec.header.nchans, dtype=np.uint8) for n in lens]
+    srv = Server([spec], hbm_budget=1 << 30, keep_dmt=True)
+    chunks = [Chunk(0, k, int(n), torch.from_numpy(v)) for k, (n, v) in enumerate(zip(lens, vals))]
+    for c in chunks:
+        srv.submit(c)
+    srv.drain()
+    torch.cuda.synchronize()
+    total = int(lens.sum())
+    ref = orc.dmt(np.concatenate(vals), st0.delays, spec.header.nchans, total, total - maxd)
+    got = [c.dmt.cpu().numpy() for c in chunks if c.nvalid > 0]
+    np.testing.assert_array_equal(np.concatenate(got, axis=1), ref)
+    assert chunks[0].nvalid <= 0 and chunks[1].nvalid <= 0
+    st = BeamState(spec, torch.device("cuda", 0))
+    alone = [plain_process(None, Chunk(0, k, int(n), torch.from_numpy(v)), st, keep_dmt=True)
+             for k, (n, v) in enumerate(zip(lens, vals))]
+    for a, c in zip(alone, chunks):
+        assert max(a.nvalid, 0) == max(c.nvalid, 0)
+        if c.nvalid > 0:
+            np.testing.assert_array_equal(a.dmt.cpu().numpy(), c.dmt.cpu().numpy())
