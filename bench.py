@@ -140,7 +140,9 @@ def _workload(args=None):
         # reduced case for profiling captures (never a bench value)
         g = dataclasses.replace(g, nsamps=args.nsamps or g.nsamps)
         ndm = args.ndm or ndm
-    dms = synth.dm_grid(1000.0, 1024)[np.linspace(0, 1023, ndm).astype(int)]
+    # a reduced case keeps the full grid's trial spacing (a contiguous block of trials)
+    lo = (1024 - ndm) // 2
+    dms = synth.dm_grid(1000.0, 1024)[lo:lo + ndm]
     delays = np.atleast_2d(g.delays(dms)).astype(np.int32)
     return g, dms, delays
 

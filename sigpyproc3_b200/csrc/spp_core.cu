@@ -88,9 +88,10 @@ static Variant mk(int single) {
 // Bit-sliced counters hold sums below 2^kBitLevels.
 constexpr int kBitLevels = 14;
 
-template <int NB, int P, int DW, int TW, int STAGES>
+template <int NB, int P, int DW, int TW, int STAGES, int SLAB = 64>
 static Variant mkb() {
-  return Variant{NB, 0, P, DW, TW, 64, STAGES, &k_dmt_bits<NB, P, DW, TW, STAGES, kBitLevels>, 0, 1};
+  return Variant{NB, 0, P, DW, TW, SLAB, STAGES,
+                 &k_dmt_bits<NB, P, DW, TW, STAGES, kBitLevels, SLAB>, 0, 1};
 }
 
 #define SPP_INT_VARIANTS(NB)                    \
@@ -100,8 +101,9 @@ static Variant mkb() {
 static const std::vector<Variant>& variants() {
   static const std::vector<Variant> v = {
       // bit-sliced (1- and 2-bit data)
-      mkb<2, 2, 8, 1, 2>(), mkb<2, 1, 8, 1, 3>(), mkb<2, 2, 16, 1, 2>(), mkb<2, 2, 4, 2, 2>(),
-      mkb<1, 2, 8, 1, 2>(), mkb<1, 1, 8, 1, 3>(), mkb<1, 2, 16, 1, 2>(),
+      mkb<2, 2, 8, 1, 2>(), mkb<2, 2, 8, 1, 3, 32>(), mkb<2, 2, 8, 1, 2, 32>(),
+      mkb<2, 4, 8, 1, 2, 32>(), mkb<2, 2, 16, 1, 2, 32>(), mkb<2, 1, 8, 1, 3>(),
+      mkb<1, 2, 8, 1, 2>(), mkb<1, 2, 8, 1, 3, 32>(), mkb<1, 4, 8, 1, 2, 32>(),
       SPP_INT_VARIANTS(1),
       SPP_INT_VARIANTS(2),
       SPP_INT_VARIANTS(4),
@@ -137,7 +139,7 @@ static int slot_words(const Variant& v, int32_t span) {
 }
 
 static int64_t smem_bytes(const Variant& v, int slot_w) {
-  if (v.planes) return v.STAGES * bits_stage_bytes(v.nb, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
+  if (v.planes) return v.STAGES * bits_stage_bytes(v.nb, v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
   return v.STAGES * dmt_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
 }
 

@@ -846,31 +846,101 @@ struct BitCounter {
   }
 };
 
-template <int NB, int P, int DW, int TW, int STAGES>
+template <int NB, int P, int DW, int TW, int SLAB>
 struct BitsShape {
-  static constexpr int kSlab = 64;
   static constexpr int kNwc = DW * TW;
   static constexpr int kThreads = (kNwc + 1) * 32;
   static constexpr int kT = TW * 32 * P * 32;  // samples per CTA tile
 };
 
-__host__ __device__ constexpr int64_t bits_stage_bytes(int nb, int slot_w, int dw) {
-  return (int64_t)64 * nb * slot_w * 4 + (int64_t)dw * 64 * 4 + 64 * 4;
+// Shared memory per stage: SLAB channels x NB plane rows x slot_w words, plus
+// DW x SLAB tile-relative sample offsets.
+__host__ __device__ constexpr int64_t bits_stage_bytes(int nb, int slab, int slot_w, int dw) {
+  return (int64_t)slab * nb * slot_w * 4 + (int64_t)dw * slab * 4;
 }
 
-template <int NB, int P, int DW, int TW, int STAGES, int L>
-__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, STAGES>::kThreads)
+// One slab of SLAB channels through the carry-save network.  FULL: all
+// channels present (no predicates); otherwise channels >= nc add zeros.
+template <int NB, int P, int L, int SLAB, bool FULL>
+__device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t* __restrict__ sd,
+                                          const int32_t* __restrict__ off, int nc, int slot_w,
+                                          int wbase) {
+  constexpr int NMID = SLAB / 16;
+  uint32_t cmid[NMID][P];
+#pragma unroll
+  for (int m = 0; m < NMID; ++m) {  // 16 channels
+    uint32_t cq[4][P];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {    // 4 channels
+      uint32_t x[NB][4][P];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j = 16 * m + 4 * i + q;
+        const bool live = FULL || j < nc;
+        const int o = live ? off[j] : 0;
+        const int sh = o & 31;
+        const uint32_t* base = sd + j * NB * slot_w + (o >> 5) + wbase;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+#pragma unroll
+          for (int p = 0; p < P; ++p) {
+            uint32_t lo = 0u, hi = 0u;
+            if (live) {
+              lo = base[b * slot_w + 32 * p];
+              hi = base[b * slot_w + 32 * p + 1];
+            }
+            x[b][q][p] = __funnelshift_r(lo, hi, sh);
+          }
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        if constexpr (NB == 2) {
+          const uint32_t lo[4] = {x[0][0][p], x[0][1][p], x[0][2][p], x[0][3][p]};
+          const uint32_t hi[4] = {x[NB - 1][0][p], x[NB - 1][1][p], x[NB - 1][2][p],
+                                  x[NB - 1][3][p]};
+          cnt.quad2(p, lo, hi, cq[i][p]);  // weight 16
+        } else {
+          const uint32_t v[4] = {x[0][0][p], x[0][1][p], x[0][2][p], x[0][3][p]};
+          cnt.quad1(p, v, cq[i][p]);       // weight 4
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const uint32_t w4[4] = {cq[0][p], cq[1][p], cq[2][p], cq[3][p]};
+      cnt.fold4(p, NB == 2 ? 4 : 2, w4, cmid[m][p]);  // weight 64 (2-bit) / 16 (1-bit)
+    }
+  }
+  constexpr int LM = NB == 2 ? 6 : 4;  // level of the per-16-channel carries
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    if constexpr (NMID == 4) {
+      const uint32_t w4[4] = {cmid[0][p], cmid[1][p], cmid[2][p], cmid[3][p]};
+      uint32_t top;
+      cnt.fold4(p, LM, w4, top);
+      cnt.ripple(p, LM + 2, top);
+    } else {
+      uint32_t top;
+      csa(cnt.A[p][LM], cmid[0][p], cmid[1][p], top);
+      cnt.ripple(p, LM + 1, top);
+    }
+  }
+}
+
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB>
+__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads)
 k_dmt_bits(const DmtArgs a) {
-  using Sh = BitsShape<NB, P, DW, TW, STAGES>;
-  constexpr int SLAB = Sh::kSlab;
+  using Sh = BitsShape<NB, P, DW, TW, SLAB>;
   constexpr int NWC = Sh::kNwc;
   constexpr int T = Sh::kT;
+  constexpr int JJ = (SLAB + 31) / 32;
+  static_assert(SLAB == 32 || SLAB == 64, "slab of 32 or 64 channels");
 
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
-  int32_t* sdel = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * NB * a.slot_w);
-  int32_t* sbase = sdel + STAGES * DW * SLAB;
-  uint64_t* full = reinterpret_cast<uint64_t*>(sbase + STAGES * SLAB);
+  int32_t* soff = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * NB * a.slot_w);
+  uint64_t* full = reinterpret_cast<uint64_t*>(soff + STAGES * DW * SLAB);
   uint64_t* empty = full + STAGES;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -889,41 +959,53 @@ k_dmt_bits(const DmtArgs a) {
   __syncthreads();
 
   if (warp == NWC) {
+    // producer: delays -> staged window start (16-B aligned word) and each DM
+    // row's sample offset within the staged window
     const uint32_t* planar = static_cast<const uint32_t*>(a.planar);
     for (int k = 0; k < nslab; ++k) {
       const int s = k % STAGES;
-      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1, a.status)) break;
       const int c0 = k * SLAB;
       const int nc = min(SLAB, a.nchans - c0);
-      int64_t ws_reg[2];
+      int32_t dv[JJ][DW];
+      int32_t mn[JJ], mx[JJ];
+      // the delay loads do not depend on the slot: issue them before waiting
 #pragma unroll
-      for (int jj = 0; jj < 2; ++jj) {
+      for (int jj = 0; jj < JJ; ++jj) {
+        const int j = lane + jj * 32;
+        mn[jj] = INT32_MAX;
+        mx[jj] = INT32_MIN;
+#pragma unroll
+        for (int i = 0; i < DW; ++i) {
+          int32_t d = 0;
+          if (j < nc) {
+            const int dm = min(dm0 + i, a.ndm - 1);
+            d = a.sign * __ldg(a.delays + (int64_t)dm * a.dpitch + c0 + j);
+            if (d < a.dlo || d > a.dhi) {
+              dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)(c0 + j));
+              d = min(max(d, a.dlo), a.dhi);
+            }
+          }
+          dv[jj][i] = d;
+          mn[jj] = min(mn[jj], d);
+          mx[jj] = max(mx[jj], d);
+        }
+      }
+      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1, a.status)) break;
+      int64_t ws_reg[JJ];
+#pragma unroll
+      for (int jj = 0; jj < JJ; ++jj) {
         const int j = lane + jj * 32;
         ws_reg[jj] = 0;
         if (j < nc) {
-          const int c = c0 + j;
-          int32_t dv[DW];
-          int32_t mn = INT32_MAX, mx = INT32_MIN;
-#pragma unroll
-          for (int i = 0; i < DW; ++i) {
-            const int dm = min(dm0 + i, a.ndm - 1);
-            int32_t d = a.sign * __ldg(a.delays + (int64_t)dm * a.dpitch + c);
-            if (d < a.dlo || d > a.dhi) {
-              dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)c);
-              d = min(max(d, a.dlo), a.dhi);
-            }
-            dv[i] = d;
-            mn = min(mn, d);
-            mx = max(mx, d);
+          if (mx[jj] - mn[jj] > a.span_max) {
+            dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)(c0 + j) | 0x80000000u);
+            mx[jj] = mn[jj] + a.span_max;
           }
-          if (mx - mn > a.span_max) {
-            dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)c | 0x80000000u);
-            mx = mn + a.span_max;
-          }
+          const int64_t ws = ((t0 + mn[jj] + a.halo) / 32) & ~int64_t(3);
+          const int32_t base = (int32_t)(ws * 32 - a.halo - t0);
 #pragma unroll
-          for (int i = 0; i < DW; ++i) sdel[(s * DW + i) * SLAB + j] = min(dv[i], mx);
-          const int64_t ws = ((t0 + mn + a.halo) / 32) & ~int64_t(3);
-          sbase[s * SLAB + j] = (int32_t)(ws * 32 - a.halo - t0);
+          for (int i = 0; i < DW; ++i)
+            soff[(s * DW + i) * SLAB + j] = min(dv[jj][i], mx[jj]) - base;
           ws_reg[jj] = ws;
         }
       }
@@ -931,7 +1013,7 @@ k_dmt_bits(const DmtArgs a) {
       if (lane == 0) mbar_arrive_expect_tx(&full[s], (uint32_t)nc * NB * a.slot_w * 4u);
       __syncwarp();
 #pragma unroll
-      for (int jj = 0; jj < 2; ++jj) {
+      for (int jj = 0; jj < JJ; ++jj) {
         const int j = lane + jj * 32;
         if (j < nc) {
 #pragma unroll
@@ -948,7 +1030,7 @@ k_dmt_bits(const DmtArgs a) {
   // consumers: warp (dmw, tw); thread words w = tw*32*P + lane + 32*p
   const int dmw = warp / TW, tw = warp % TW;
   const int dm = dm0 + dmw;
-  const int wbase = tw * 32 * P + lane;  // word index of p = 0 within the tile
+  const int wbase = tw * 32 * P + lane;
   BitCounter<P, L> cnt;
   cnt.zero();
   bool ok = true;
@@ -957,63 +1039,9 @@ k_dmt_bits(const DmtArgs a) {
     if (!mbar_wait(&full[s], (k / STAGES) & 1, a.status)) { ok = false; break; }
     const int nc = min(SLAB, a.nchans - k * SLAB);
     const uint32_t* sd = sdata + (int64_t)s * SLAB * NB * a.slot_w;
-    const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
-    const int32_t* bs = sbase + s * SLAB;
-    uint32_t c64[4][P];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {        // 16 channels
-      uint32_t cm[4][P];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {      // 4 channels
-        uint32_t x[NB][4][P];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int j = 16 * m + 4 * i + q;
-          const bool live = j < nc;
-          const int o = live ? (dl[j] - bs[j]) : 0;
-          const int wo = o >> 5, sh = o & 31;
-#pragma unroll
-          for (int b = 0; b < NB; ++b) {
-            const uint32_t* row = sd + (j * NB + b) * a.slot_w + wo + wbase;
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-              const uint32_t lo = live ? row[32 * p] : 0u;
-              const uint32_t hi = live ? row[32 * p + 1] : 0u;
-              x[b][q][p] = __funnelshift_r(lo, hi, sh);
-            }
-          }
-        }
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-          if constexpr (NB == 2) {
-            const uint32_t lo[4] = {x[0][0][p], x[0][1][p], x[0][2][p], x[0][3][p]};
-            const uint32_t hi[4] = {x[NB - 1][0][p], x[NB - 1][1][p], x[NB - 1][2][p], x[NB - 1][3][p]};
-            cnt.quad2(p, lo, hi, cm[i][p]);   // weight 16
-          } else {
-            const uint32_t v[4] = {x[0][0][p], x[0][1][p], x[0][2][p], x[0][3][p]};
-            cnt.quad1(p, v, cm[i][p]);        // weight 4
-          }
-        }
-      }
-#pragma unroll
-      for (int p = 0; p < P; ++p) {
-        const uint32_t w4[4] = {cm[0][p], cm[1][p], cm[2][p], cm[3][p]};
-        if constexpr (NB == 2) cnt.fold4(p, 4, w4, c64[m][p]);   // -> weight 64
-        else cnt.fold4(p, 2, w4, c64[m][p]);                      // -> weight 16
-      }
-    }
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-      const uint32_t w4[4] = {c64[0][p], c64[1][p], c64[2][p], c64[3][p]};
-      uint32_t top;
-      if constexpr (NB == 2) {
-        cnt.fold4(p, 6, w4, top);  // weight 256
-        cnt.ripple(p, 8, top);
-      } else {
-        cnt.fold4(p, 4, w4, top);  // weight 64
-        cnt.ripple(p, 6, top);
-      }
-    }
+    const int32_t* off = soff + (s * DW + dmw) * SLAB;
+    if (nc == SLAB) bits_slab<NB, P, L, SLAB, true>(cnt, sd, off, nc, a.slot_w, wbase);
+    else bits_slab<NB, P, L, SLAB, false>(cnt, sd, off, nc, a.slot_w, wbase);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
