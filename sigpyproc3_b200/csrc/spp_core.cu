@@ -14,6 +14,10 @@
 
 namespace spp {
 
+int launch_single8(const uint8_t* raw, int64_t nchans, int64_t nsamps, const int32_t* delays,
+                   int32_t dlo, int32_t dhi, float* out, int64_t out_start, int64_t nvalid,
+                   uint32_t* status, cudaStream_t st);
+
 static thread_local char g_err[1024] = "";
 
 int fail(int code, const char* fmt, ...) {
@@ -354,6 +358,12 @@ int spp_dedisperse(const void* in, int nbits, int bitorder, int64_t nchans, int6
     return fail(SPP_ERR_ALIGN, "workspace must be 256-B aligned");
   cudaStream_t st = as_stream(stream);
   uint8_t* ws = static_cast<uint8_t*>(workspace);
+  if (nbits == 8) {
+    // one pass over the raw block when the delay spread fits the staging buffer
+    rc = launch_single8(static_cast<const uint8_t*>(in), nchans, nsamps, delays, delay_min,
+                        delay_max, out, out_start, g.nvalid, reinterpret_cast<uint32_t*>(ws), st);
+    if (rc != SPP_ERR_UNSUPPORTED) return rc;
+  }
   void* planar = ws + kStatusBytes;
   rc = launch_corner_turn(nbits, in, bitorder, nchans, nsamps, g, planar, st);
   if (rc) return rc;
