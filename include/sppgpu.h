@@ -260,7 +260,8 @@ typedef struct spp_dmt_item {
 } spp_dmt_item;           /* 112 bytes */
 
 int spp_wl_num_variants(int nbits, int acc);
-/* cfg[8] = {R, DW, TW, SLAB, STAGES, T (samples per item), threads, samples/word} */
+/* cfg[8] = {R, DW, TW, SLAB, STAGES, T (samples per item), threads,
+ *           samples per word | 256 if the variant is bit-sliced} */
 int spp_wl_describe(int nbits, int acc, int variant, int32_t* cfg);
 int32_t spp_wl_slot_words(int nbits, int acc, int variant, int32_t span_max);
 int64_t spp_wl_smem_bytes(int nbits, int acc, int variant, int32_t slot_w);
@@ -273,10 +274,25 @@ int32_t spp_wl_default_ctas(int nbits, int acc, int variant, int32_t slot_w);
 /* Planar layout for offsets in [omin, omax] and nvalid outputs tiled by tile_T. */
 int spp_planar_layout(int nbits, int64_t tile_T, int64_t nvalid, int32_t omin,
                       int32_t omax, int32_t slot_w, int64_t* halo, int64_t* pitch_w);
+/* Planar layout and corner turn matching a work-list variant: bit-sliced
+ * variants (1/2-bit data) use nbits bit-plane rows per channel
+ * (*rows_per_chan = nbits), the others one packed row per channel. */
+int spp_wl_planar_layout(int nbits, int acc, int variant, int64_t nvalid, int32_t omin,
+                         int32_t omax, int32_t slot_w, int64_t* halo, int64_t* pitch_w,
+                         int64_t* rows_per_chan);
+int spp_wl_corner_turn(int nbits, int acc, int variant, const void* in, int bitorder,
+                       int64_t nchans, int64_t nsamps, int64_t halo, void* planar,
+                       int64_t pitch_w, void* stream);
 /* Raw time-major block -> planar rows (channel-major, time packed in words). */
 int spp_corner_turn(const void* in, int nbits, int bitorder, int64_t nchans,
                     int64_t nsamps, int64_t halo, void* planar, int64_t pitch_w,
                     void* stream);
+
+/* Self-test of the device-side failure path: launches one CTA whose mbarrier
+ * wait can never complete; after limit_ns (<= 1 s) the bounded wait gives up
+ * and sets SPP_DEV_TIMEOUT (bit 0) in status[0] (a device status block, as
+ * read by spp_status_read).  No trap, no fault: the context stays usable. */
+int spp_selftest_wait_timeout(uint32_t* status, uint64_t limit_ns, void* stream);
 
 /* ---- Synthetic inputs (benchmark / test data; no reference counterpart) -------
  * Counter-based generators: element i depends only on (seed, start + i)

@@ -80,8 +80,11 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_wl_smem_bytes": ([_int, _int, _int, _i32], _i64),
     "spp_wl_launch": ([_int, _int, _int, _p, _i32, _i32, _p, _p, _i32, _p], _int),
     "spp_wl_default_ctas": ([_int, _int, _int, _i32], _i32),
+    "spp_wl_planar_layout": ([_int, _int, _int, _i64, _i32, _i32, _i32, _p, _p, _p], _int),
+    "spp_wl_corner_turn": ([_int, _int, _int, _p, _int, _i64, _i64, _i64, _p, _i64, _p], _int),
     "spp_planar_layout": ([_int, _i64, _i64, _i32, _i32, _i32, _p, _p], _int),
     "spp_corner_turn": ([_p, _int, _int, _i64, _i64, _i64, _p, _i64, _p], _int),
+    "spp_selftest_wait_timeout": ([_p, ctypes.c_uint64, _p], _int),
     "spp_synth_uniform_bytes": ([_p, _i64, _i64, ctypes.c_uint64, _p], _int),
     "spp_synth_gauss_u8": ([_p, _i64, _i64, ctypes.c_uint64, _p, _p], _int),
     "spp_synth_gauss_f32": ([_p, _i64, _i64, ctypes.c_uint64, ctypes.c_float, ctypes.c_float, _p],

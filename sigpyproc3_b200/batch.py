@@ -29,7 +29,10 @@ ITEM_DTYPE = np.dtype({
 def variant_cfg(nbits: int, acc: int, variant: int) -> dict:
     cfg = (ctypes.c_int32 * 8)()
     _lib.check(_lib.load().spp_wl_describe(nbits, acc, variant, cfg))
-    return dict(zip(("R", "DW", "TW", "SLAB", "STAGES", "T", "threads", "spw"), list(cfg)))
+    d = dict(zip(("R", "DW", "TW", "SLAB", "STAGES", "T", "threads", "spw"), list(cfg)))
+    d["planes"] = d["spw"] >> 8
+    d["spw"] &= 0xFF
+    return d
 
 
 def num_variants(nbits: int, acc: int = _lib.ACC_KAHAN32) -> int:
@@ -116,6 +119,23 @@ class WorkList:
         rec["dhi"] = dhi
         rec["out_kind"] = out_kind
         self._rows.append(rec)
+
+    def layout(self, nvalid: int, omin: int, omax: int, slot_w: int | None = None):
+        """(halo, pitch_w, rows per channel) of planar rows for this variant."""
+        halo, pitch, rows = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _lib.check(_lib.load().spp_wl_planar_layout(
+            self.nbits, self.acc, self.variant, nvalid, omin, omax,
+            self.slot_words() if slot_w is None else slot_w, ctypes.byref(halo),
+            ctypes.byref(pitch), ctypes.byref(rows)))
+        return halo.value, pitch.value, rows.value
+
+    def corner_turn(self, raw: torch.Tensor, bitorder: int, nchans: int, nsamps: int, halo: int,
+                    planar: torch.Tensor, pitch_w: int,
+                    stream: torch.cuda.Stream | None = None) -> None:
+        st = (stream or torch.cuda.current_stream(raw.device)).cuda_stream
+        _lib.check(_lib.load().spp_wl_corner_turn(self.nbits, self.acc, self.variant,
+                                                  raw.data_ptr(), bitorder, nchans, nsamps, halo,
+                                                  planar.data_ptr(), pitch_w, st))
 
     def slot_words(self, span: int | None = None) -> int:
         return int(_lib.load().spp_wl_slot_words(self.nbits, self.acc, self.variant,

@@ -11,11 +11,18 @@ namespace spp {
 struct WlVariant {
   int nb, acc, R, DW, TW, SLAB, STAGES;
   void (*fn)(const WlArgs);
+  int planes;  // 1: bit-sliced over bit-plane rows (R = words per thread)
 };
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
 static WlVariant mkwl() {
-  return WlVariant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt_wl<NB, R, DW, TW, SLAB, STAGES, ACC>};
+  return WlVariant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt_wl<NB, R, DW, TW, SLAB, STAGES, ACC>, 0};
+}
+
+template <int NB, int P, int DW, int TW, int STAGES, int SLAB>
+static WlVariant mkwlb() {
+  return WlVariant{NB, 0, P, DW, TW, SLAB, STAGES,
+                   &k_dmt_bits_wl<NB, P, DW, TW, STAGES, 14, SLAB>, 1};
 }
 
 #define SPP_WL_INT(NB)                                                                  \
@@ -24,6 +31,8 @@ static WlVariant mkwl() {
 
 static const std::vector<WlVariant>& wl_variants() {
   static const std::vector<WlVariant> v = {
+      mkwlb<1, 2, 8, 1, 2, 64>(), mkwlb<1, 2, 8, 1, 3, 32>(),
+      mkwlb<2, 2, 8, 1, 2, 64>(), mkwlb<2, 2, 8, 1, 3, 32>(),
       SPP_WL_INT(1), SPP_WL_INT(2), SPP_WL_INT(4), SPP_WL_INT(8), SPP_WL_INT(16),
       mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_KAHAN32>(), mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_KAHAN32>(),
       mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_F64>(),     mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_F64>(),
@@ -42,18 +51,20 @@ static const WlVariant* wl_find(int nbits, int acc, int variant) {
 }
 
 static int spw_of_nb(int nb) { return nb == 32 ? 1 : 32 / nb; }
+static int spw_wl(const WlVariant& v) { return v.planes ? 32 : spw_of_nb(v.nb); }
 
-static int64_t wl_T(const WlVariant& v) { return (int64_t)v.TW * 32 * v.R * spw_of_nb(v.nb); }
+static int64_t wl_T(const WlVariant& v) { return (int64_t)v.TW * 32 * v.R * spw_wl(v); }
 
 static int32_t wl_slot(const WlVariant& v, int32_t span) {
-  const int spw = spw_of_nb(v.nb);
+  const int spw = spw_wl(v);
   const int64_t w = wl_T(v) / spw + ceil_div(std::max<int32_t>(span, 0), spw) + 6 + v.R;
   return (int32_t)round_up(w, 4);
 }
 
 static int64_t wl_smem(const WlVariant& v, int32_t slot_w) {
-  return (int64_t)v.STAGES * dmt_stage_bytes(v.SLAB, slot_w, v.DW) + 16 * v.STAGES + 8 +
-         2 * v.STAGES * 8;
+  const int64_t stage = v.planes ? bits_stage_bytes(v.nb, v.SLAB, slot_w, v.DW)
+                                 : dmt_stage_bytes(v.SLAB, slot_w, v.DW);
+  return (int64_t)v.STAGES * stage + 16 * v.STAGES + 8 + 2 * v.STAGES * 8;
 }
 
 static inline cudaStream_t stq(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -77,7 +88,7 @@ int spp_wl_describe(int nbits, int acc, int variant, int32_t* cfg) {
   cfg[0] = v->R; cfg[1] = v->DW; cfg[2] = v->TW; cfg[3] = v->SLAB; cfg[4] = v->STAGES;
   cfg[5] = (int32_t)wl_T(*v);
   cfg[6] = (v->DW * v->TW + 1) * 32;
-  cfg[7] = spw_of_nb(nbits);
+  cfg[7] = spw_wl(*v) | (v->planes << 8);
   return SPP_OK;
 }
 
@@ -190,3 +201,41 @@ extern "C" int32_t spp_wl_default_ctas(int nbits, int acc, int variant, int32_t 
     return -1;
   return std::max(1, sms * std::max(per, 1));
 }
+
+extern "C" {
+
+int spp_wl_planar_layout(int nbits, int acc, int variant, int64_t nvalid, int32_t omin,
+                         int32_t omax, int32_t slot_w, int64_t* halo, int64_t* pitch_w,
+                         int64_t* rows_per_chan) {
+  const WlVariant* v = wl_find(nbits, acc, variant);
+  if (!v || !halo || !pitch_w || !rows_per_chan || slot_w <= 0) return fail(SPP_ERR_ARG, "bad layout arguments");
+  const int spw = spw_wl(*v);
+  const int64_t T = wl_T(*v);
+  *halo = round_up(std::max<int64_t>(0, -(int64_t)omin), 4 * spw);
+  const int64_t ntiles = ceil_div(std::max<int64_t>(nvalid, 1), T);
+  const int64_t last = ntiles * T + std::max<int64_t>(0, omax) + *halo;
+  *pitch_w = round_up(ceil_div(last, spw) + slot_w + 8, 4);
+  *rows_per_chan = v->planes ? v->nb : 1;
+  return SPP_OK;
+}
+
+int spp_wl_corner_turn(int nbits, int acc, int variant, const void* in, int bitorder,
+                       int64_t nchans, int64_t nsamps, int64_t halo, void* planar,
+                       int64_t pitch_w, void* stream) {
+  const WlVariant* v = wl_find(nbits, acc, variant);
+  if (!v) return fail(SPP_ERR_ARG, "no work-list variant %d for nbits=%d", variant, nbits);
+  if (!v->planes) return spp_corner_turn(in, nbits, bitorder, nchans, nsamps, halo, planar, pitch_w, stream);
+  if (!in || !planar || nchans <= 0 || nsamps <= 0 || (pitch_w & 3) || halo < 0 || (nchans * nbits) % 8)
+    return fail(SPP_ERR_ARG, "bad corner-turn arguments");
+  dim3 grid((unsigned)ceil_div(nchans, kCtChans), (unsigned)std::min<int64_t>(ceil_div(pitch_w, kCtWords), 65535));
+  const uint8_t* raw = static_cast<const uint8_t*>(in);
+  uint32_t* pl = static_cast<uint32_t*>(planar);
+  cudaStream_t st = stq(stream);
+  if (nbits == 1)
+    k_corner_turn_planes<1><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
+  else
+    k_corner_turn_planes<2><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
+  return cuda_status(cudaGetLastError(), "plane corner turn launch");
+}
+
+}  // extern "C"

@@ -104,6 +104,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
   }
 }
 
+// Bounded wait with an explicit limit (nanoseconds), for the self-test.
+__device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, uint32_t* status,
+                                             uint64_t limit_ns) {
+  const uint64_t t0 = global_timer_ns();
+  for (uint32_t i = 0;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 0 && global_timer_ns() - t0 > limit_ns) {
+      dev_flag(status, SPP_DEV_TIMEOUT, i);
+      return false;
+    }
+  }
+}
+
 // 1-D bulk copy global -> shared, completion signalled on `bar` (transaction
 // bytes).  dst/src 16-B aligned, bytes a multiple of 16.  Plain (no cluster
 // multicast) copy of this GPU's own memory.

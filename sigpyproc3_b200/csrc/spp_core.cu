@@ -563,27 +563,36 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
     delete p;
     return fail(SPP_ERR_DELAY, "roll mode needs |delay| < nsamps");
   }
-  // candidates
+  // candidates; the delay spread of DM tiles is computed once per tile height
   const auto& vs = variants();
+  std::vector<std::pair<int, int32_t>> span_of_dw;
+  auto tile_span = [&](int dw) -> int32_t {
+    for (auto& e : span_of_dw)
+      if (e.first == dw) return e.second;
+    int32_t span = 0;
+    std::vector<int32_t> mn(nchans), mx(nchans);
+    for (int64_t d0 = 0; d0 < ndm; d0 += dw) {
+      const int64_t d1 = std::min<int64_t>(ndm, d0 + dw);
+      std::copy(delays_host + d0 * nchans, delays_host + (d0 + 1) * nchans, mn.begin());
+      std::copy(mn.begin(), mn.end(), mx.begin());
+      for (int64_t d = d0 + 1; d < d1; ++d) {
+        const int32_t* row = delays_host + d * nchans;
+        for (int64_t c = 0; c < nchans; ++c) {
+          mn[c] = std::min(mn[c], row[c]);
+          mx[c] = std::max(mx[c], row[c]);
+        }
+      }
+      for (int64_t c = 0; c < nchans; ++c) span = std::max(span, mx[c] - mn[c]);
+    }
+    span_of_dw.emplace_back(dw, span);
+    return span;
+  };
   for (int i = 0; i < (int)vs.size(); ++i) {
     const Variant& v = vs[i];
     if (v.nb != nbits || (nbits == 32 && v.acc != acc)) continue;
     if (ndm == 1 ? !v.single : v.single) continue;
     if (v.planes && nchans * ((1 << nbits) - 1) >= (1 << kBitLevels)) continue;
-    // span for tiles of v.DW consecutive DMs
-    int32_t span = 0;
-    for (int64_t d0 = 0; d0 < ndm; d0 += v.DW) {
-      const int64_t d1 = std::min<int64_t>(ndm, d0 + v.DW);
-      for (int64_t c = 0; c < nchans; ++c) {
-        int32_t mn = INT32_MAX, mx = INT32_MIN;
-        for (int64_t d = d0; d < d1; ++d) {
-          const int32_t x = delays_host[d * nchans + c];
-          mn = std::min(mn, x);
-          mx = std::max(mx, x);
-        }
-        span = std::max(span, mx - mn);
-      }
-    }
+    const int32_t span = tile_span(v.DW);
     if (smem_bytes(v, slot_words(v, span)) > kMaxSmem) continue;
     p->cands.push_back(i);
     p->spans.push_back(span);

@@ -1145,4 +1145,173 @@ k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t ns
     __syncthreads();
   }
 }
+
+// ----------------------------------------------------------------------------
+// Persistent work-list version of the bit-sliced kernel (same items as
+// k_dmt_wl; planar rows are bit-plane rows, NB per channel).
+// ----------------------------------------------------------------------------
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB>
+__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads)
+k_dmt_bits_wl(const WlArgs w) {
+  using Sh = BitsShape<NB, P, DW, TW, SLAB>;
+  constexpr int NWC = Sh::kNwc;
+  constexpr int JJ = (SLAB + 31) / 32;
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
+  int32_t* soff = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * NB * w.slot_w);
+  int32_t* stag = soff + STAGES * DW * SLAB;  // per stage: item, slab, nslab, pad
+  uint64_t* full = reinterpret_cast<uint64_t*>(stag + 4 * STAGES);
+  uint64_t* empty = full + STAGES;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NWC);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == NWC) {
+    uint32_t gk = 0;
+    bool ok = true;
+    while (ok) {
+      int it_idx = 0;
+      if (lane == 0) it_idx = atomicAdd(w.counter, 1);
+      it_idx = __shfl_sync(0xffffffffu, it_idx, 0);
+      if (it_idx >= w.nitems) break;
+      const DmtItem it = w.items[it_idx];
+      const uint32_t* planar = static_cast<const uint32_t*>(it.planar);
+      const int nslab = (it.nchans + SLAB - 1) / SLAB;
+      for (int k = 0; k < nslab; ++k, ++gk) {
+        const int s = gk % STAGES;
+        const int c0 = k * SLAB;
+        const int nc = min(SLAB, it.nchans - c0);
+        int32_t dv[JJ][DW];
+        int32_t mn[JJ], mx[JJ];
+#pragma unroll
+        for (int jj = 0; jj < JJ; ++jj) {
+          const int j = lane + jj * 32;
+          mn[jj] = INT32_MAX;
+          mx[jj] = INT32_MIN;
+#pragma unroll
+          for (int i = 0; i < DW; ++i) {
+            int32_t d = 0;
+            if (j < nc) {
+              const int r = min(i, it.nrows - 1);
+              d = it.sign * __ldg(it.delays + (int64_t)r * it.dpitch + c0 + j);
+              if (d < it.dlo || d > it.dhi) {
+                dev_flag(w.status, SPP_DEV_RANGE, (uint32_t)(c0 + j));
+                d = min(max(d, it.dlo), it.dhi);
+              }
+            }
+            dv[jj][i] = d;
+            mn[jj] = min(mn[jj], d);
+            mx[jj] = max(mx[jj], d);
+          }
+        }
+        if (gk >= STAGES && !mbar_wait(&empty[s], ((gk / STAGES) - 1) & 1, w.status)) {
+          ok = false;
+          break;
+        }
+        int64_t ws_reg[JJ];
+#pragma unroll
+        for (int jj = 0; jj < JJ; ++jj) {
+          const int j = lane + jj * 32;
+          ws_reg[jj] = 0;
+          if (j < nc) {
+            if (mx[jj] - mn[jj] > it.span_max) {
+              dev_flag(w.status, SPP_DEV_RANGE, (uint32_t)(c0 + j) | 0x80000000u);
+              mx[jj] = mn[jj] + it.span_max;
+            }
+            const int64_t ws = ((it.t0 + mn[jj] + it.halo) / 32) & ~int64_t(3);
+            const int32_t base = (int32_t)(ws * 32 - it.halo - it.t0);
+#pragma unroll
+            for (int i = 0; i < DW; ++i)
+              soff[(s * DW + i) * SLAB + j] = min(dv[jj][i], mx[jj]) - base;
+            ws_reg[jj] = ws;
+          }
+        }
+        if (lane == 0) {
+          stag[4 * s + 0] = it_idx;
+          stag[4 * s + 1] = k;
+          stag[4 * s + 2] = nslab;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(&full[s], (uint32_t)nc * NB * w.slot_w * 4u);
+        __syncwarp();
+#pragma unroll
+        for (int jj = 0; jj < JJ; ++jj) {
+          const int j = lane + jj * 32;
+          if (j < nc) {
+#pragma unroll
+            for (int b = 0; b < NB; ++b)
+              bulk_g2s(sdata + (((int64_t)s * SLAB + j) * NB + b) * w.slot_w,
+                       planar + ((int64_t)(c0 + j) * NB + b) * it.pitch_w + ws_reg[jj],
+                       w.slot_w * 4u, &full[s]);
+          }
+        }
+      }
+    }
+    if (ok) {
+      const int s = gk % STAGES;
+      if (gk < STAGES || mbar_wait(&empty[s], ((gk / STAGES) - 1) & 1, w.status)) {
+        if (lane == 0) {
+          stag[4 * s + 0] = -1;
+          mbar_arrive(&full[s]);
+        }
+      }
+    }
+    return;
+  }
+
+  const int dmw = warp / TW, tw = warp % TW;
+  const int wbase = tw * 32 * P + lane;
+  BitCounter<P, L> cnt;
+  cnt.zero();
+  DmtItem it{};
+  for (uint32_t gk = 0;; ++gk) {
+    const int s = gk % STAGES;
+    if (!mbar_wait(&full[s], (gk / STAGES) & 1, w.status)) return;
+    const int it_idx = stag[4 * s + 0];
+    if (it_idx < 0) return;
+    const int k = stag[4 * s + 1], nslab = stag[4 * s + 2];
+    if (k == 0) {
+      it = w.items[it_idx];
+      cnt.zero();
+    }
+    const int nc = min(SLAB, it.nchans - k * SLAB);
+    const uint32_t* sd = sdata + (int64_t)s * SLAB * NB * w.slot_w;
+    const int32_t* off = soff + (s * DW + dmw) * SLAB;
+    if (nc == SLAB) bits_slab<NB, P, L, SLAB, true>(cnt, sd, off, nc, w.slot_w, wbase);
+    else bits_slab<NB, P, L, SLAB, false>(cnt, sd, off, nc, w.slot_w, wbase);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    if (k == nslab - 1 && dmw < it.nrows) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const int64_t tb = it.t0 + 32LL * (wbase + 32 * p);
+        if (it.out_kind == SPP_OUT_I32) {
+          int32_t* out = static_cast<int32_t*>(it.out) + (int64_t)dmw * it.out_stride + it.out_start;
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (tb + i < it.nvalid) out[tb + i] = (int32_t)cnt.count(p, i);
+        } else if (it.out_kind == SPP_OUT_U16) {
+          uint16_t* out = static_cast<uint16_t*>(it.out) + (int64_t)dmw * it.out_stride + it.out_start;
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (tb + i < it.nvalid) out[tb + i] = (uint16_t)min(cnt.count(p, i), 65535u);
+        } else {
+          float* out = static_cast<float*>(it.out) + (int64_t)dmw * it.out_stride + it.out_start;
+#pragma unroll
+          for (int i = 0; i < 32; ++i)
+            if (tb + i < it.nvalid) out[tb + i] = (float)cnt.count(p, i);
+        }
+      }
+    }
+  }
+}
 }  // namespace spp

@@ -85,6 +85,23 @@ __global__ void k_pulse_packed(uint8_t* __restrict__ raw, int64_t nchans, int64_
   }
 }
 
+// Self-test of the bounded-wait path: an mbarrier expecting two arrivals gets
+// one, so its phase never completes; the wait gives up after limit_ns and
+// records SPP_DEV_TIMEOUT in the status word.
+__global__ void k_wait_selftest(uint32_t* status, uint64_t limit_ns) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 2);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive(&bar);
+    mbar_wait_ns(&bar, 0, status, limit_ns);
+  }
+  __syncthreads();
+}
+
 }  // namespace spp
 
 using namespace spp;
@@ -117,6 +134,13 @@ int spp_synth_gauss_f32(float* out, int64_t start, int64_t n, uint64_t seed, flo
   const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(n, 256), 148 * 64);
   k_gauss_f32<<<blocks, 256, 0, st_of(stream)>>>(out, start, n, seed, mean, stdv);
   return cuda_status(cudaGetLastError(), "synth launch");
+}
+
+int spp_selftest_wait_timeout(uint32_t* status, uint64_t limit_ns, void* stream) {
+  if (!status) return fail(SPP_ERR_ARG, "null status");
+  if (limit_ns > 1000000000ull) return fail(SPP_ERR_ARG, "limit above one second");
+  k_wait_selftest<<<1, 32, 0, st_of(stream)>>>(status, limit_ns);
+  return cuda_status(cudaGetLastError(), "self-test launch");
 }
 
 int spp_synth_pulse_packed(uint8_t* raw, int64_t nchans, int64_t nsamps, int nbits, int bitorder,

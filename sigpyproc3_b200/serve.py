@@ -112,7 +112,8 @@ class Server:
         rows = c.nsamps + st.maxd
         cfg = variant_cfg(st.nbits, _lib.ACC_KAHAN32, self.variant)
         spw = cfg["spw"]
-        planar = st.nchans * (rows // spw + 4096) * 4
+        planes = st.nbits if cfg["planes"] else 1
+        planar = st.nchans * planes * (rows // spw + 4096) * 4
         return rows * st.row_bytes + planar + st.ndm * c.nsamps * 4
 
     # ---- API ----
@@ -177,11 +178,11 @@ class Server:
                     if c.nvalid <= 0:
                         continue
                     rows = c.nsamps + st.maxd - start_row
-                    halo, pitch = planar_layout(nbits, wl.T, c.nvalid, 0, st.maxd, slot)
-                    plen = st.nchans * pitch
+                    halo, pitch, rpc = wl.layout(c.nvalid, 0, st.maxd, slot)
+                    plen = st.nchans * rpc * pitch
                     planar = torch.empty(plen, dtype=torch.int32, device=self.device)
-                    corner_turn(raw[start_row * st.row_bytes:], nbits, st.bitorder, st.nchans, rows,
-                                halo, planar, pitch, stream=stream)
+                    wl.corner_turn(raw[start_row * st.row_bytes:], st.bitorder, st.nchans, rows,
+                                   halo, planar, pitch, stream=stream)
                     dmt = torch.empty((st.ndm, c.nvalid), dtype=torch.int32, device=self.device)
                     wl.add_job(planar_ptr=planar.data_ptr(), pitch_w=pitch, halo=halo,
                                nchans=st.nchans, delays_dev=st.delays_dev, delays_host=st.delays,

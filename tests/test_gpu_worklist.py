@@ -52,10 +52,10 @@ def test_worklist_jobs_match_oracle(torch_cuda, orc, nbits):
         outs = []
         for nchans, nsamps, vals, raw, d in jobs:
             nv = nsamps - int(d.max())
-            halo, pitch = planar_layout(nbits, wl.T, nv, 0, int(d.max()), slot)
-            planar = torch.empty(nchans * pitch, dtype=torch.int32, device="cuda")
+            halo, pitch, rpc = wl.layout(nv, 0, int(d.max()), slot)
+            planar = torch.empty(nchans * rpc * pitch, dtype=torch.int32, device="cuda")
             rawd = torch.from_numpy(raw).cuda()
-            corner_turn(rawd, nbits, _lib.BITORDER_BIG, nchans, nsamps, halo, planar, pitch)
+            wl.corner_turn(rawd, _lib.BITORDER_BIG, nchans, nsamps, halo, planar, pitch)
             dd = torch.from_numpy(d).cuda()
             out = torch.full((d.shape[0], nv), -1, dtype=torch.int32, device="cuda")
             wl.add_job(planar_ptr=planar.data_ptr(), pitch_w=pitch, halo=halo, nchans=nchans,
