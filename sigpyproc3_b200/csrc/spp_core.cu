@@ -81,21 +81,22 @@ struct Variant {
   void (*fn)(const DmtArgs);
   int single;  // 1: meant for one DM (time-split warps)
   int planes;  // 1: bit-sliced kernel over bit-plane rows (R = words per thread)
+  int slot;    // > 0: kernel compiled for exactly this slot width (words)
 };
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
 static Variant mk(int single) {
   return Variant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt<NB, R, DW, TW, SLAB, STAGES, ACC>,
-                 single, 0};
+                 single, 0, 0};
 }
 
 // Bit-sliced counters hold sums below 2^kBitLevels.
 constexpr int kBitLevels = 14;
 
-template <int NB, int P, int DW, int TW, int STAGES, int SLAB = 64>
+template <int NB, int P, int DW, int TW, int STAGES, int SLAB = 64, int SLOT = 0>
 static Variant mkb() {
   return Variant{NB, 0, P, DW, TW, SLAB, STAGES,
-                 &k_dmt_bits<NB, P, DW, TW, STAGES, kBitLevels, SLAB>, 0, 1};
+                 &k_dmt_bits<NB, P, DW, TW, STAGES, kBitLevels, SLAB, SLOT>, 0, 1, SLOT};
 }
 
 #define SPP_INT_VARIANTS(NB)                    \
@@ -105,6 +106,7 @@ static Variant mkb() {
 static const std::vector<Variant>& variants() {
   static const std::vector<Variant> v = {
       // bit-sliced (1- and 2-bit data)
+      mkb<2, 2, 8, 1, 2, 64, 80>(), mkb<2, 2, 8, 1, 2, 64, 96>(),
       mkb<2, 2, 8, 1, 2>(), mkb<2, 2, 8, 1, 3, 32>(), mkb<2, 2, 8, 1, 2, 32>(),
       mkb<2, 4, 8, 1, 2, 32>(), mkb<2, 2, 16, 1, 2, 32>(), mkb<2, 1, 8, 1, 3>(),
       mkb<1, 2, 8, 1, 2>(), mkb<1, 2, 8, 1, 3, 32>(), mkb<1, 4, 8, 1, 2, 32>(),
@@ -139,7 +141,9 @@ static inline int64_t tile_T(const Variant& v) {
 static int slot_words(const Variant& v, int32_t span) {
   const int spw = spw_v(v);
   const int64_t w = tile_T(v) / spw + ceil_div(std::max<int32_t>(span, 0), spw) + 6 + v.R;
-  return (int)round_up(w, 4);
+  const int need = (int)round_up(w, 4);
+  if (v.slot > 0) return need <= v.slot ? v.slot : -1;  // fixed-width kernels
+  return need;
 }
 
 static int64_t smem_bytes(const Variant& v, int slot_w) {
@@ -593,6 +597,7 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
     if (ndm == 1 ? !v.single : v.single) continue;
     if (v.planes && nchans * ((1 << nbits) - 1) >= (1 << kBitLevels)) continue;
     const int32_t span = tile_span(v.DW);
+    if (slot_words(v, span) < 0) continue;  // fixed slot too narrow for this table
     if (smem_bytes(v, slot_words(v, span)) > kMaxSmem) continue;
     p->cands.push_back(i);
     p->spans.push_back(span);

@@ -861,10 +861,12 @@ __host__ __device__ constexpr int64_t bits_stage_bytes(int nb, int slab, int slo
 
 // One slab of SLAB channels through the carry-save network.  FULL: all
 // channels present (no predicates); otherwise channels >= nc add zeros.
-template <int NB, int P, int L, int SLAB, bool FULL>
+template <int NB, int P, int L, int SLAB, bool FULL, int SLOT = 0>
 __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t* __restrict__ sd,
-                                          const int32_t* __restrict__ off, int nc, int slot_w,
+                                          const int32_t* __restrict__ off, int nc, int slot_rt,
                                           int wbase) {
+  // SLOT > 0: slot width known at compile time (immediate load offsets)
+  const int slot_w = SLOT > 0 ? SLOT : slot_rt;
   constexpr int NMID = SLAB / 16;
   uint32_t cmid[NMID][P];
 #pragma unroll
@@ -928,7 +930,7 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
   }
 }
 
-template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB>
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT = 0>
 __global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads)
 k_dmt_bits(const DmtArgs a) {
   using Sh = BitsShape<NB, P, DW, TW, SLAB>;
@@ -1040,8 +1042,8 @@ k_dmt_bits(const DmtArgs a) {
     const int nc = min(SLAB, a.nchans - k * SLAB);
     const uint32_t* sd = sdata + (int64_t)s * SLAB * NB * a.slot_w;
     const int32_t* off = soff + (s * DW + dmw) * SLAB;
-    if (nc == SLAB) bits_slab<NB, P, L, SLAB, true>(cnt, sd, off, nc, a.slot_w, wbase);
-    else bits_slab<NB, P, L, SLAB, false>(cnt, sd, off, nc, a.slot_w, wbase);
+    if (nc == SLAB) bits_slab<NB, P, L, SLAB, true, SLOT>(cnt, sd, off, nc, a.slot_w, wbase);
+    else bits_slab<NB, P, L, SLAB, false, SLOT>(cnt, sd, off, nc, a.slot_w, wbase);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
   }
