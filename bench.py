@@ -270,7 +270,7 @@ def run_gpu(args, rank, world, local):
         host_in = torch.empty(raw.numel(), dtype=torch.uint8).pin_memory()
         host_in.copy_(raw.cpu())
         host_out = torch.empty((delays.shape[0], nvalid), dtype=torch.int32).pin_memory()
-        blk = 262144
+        blk = args.e2e_block
         hws = workspace(plan.host_workspace_bytes(blk), dev, stream=None)
         del out
         torch.cuda.empty_cache()
@@ -448,6 +448,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-block", type=int, default=65536,
+                    help="output samples per host-streaming block in the e2e leg")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="fix the kernel variant")
     ap.add_argument("--workload", choices=["c2", "c3", "c4", "c1", "c5"], default="c2")

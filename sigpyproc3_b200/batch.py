@@ -41,12 +41,13 @@ def num_variants(nbits: int, acc: int = _lib.ACC_KAHAN32) -> int:
 
 def tile_span(delays: np.ndarray, dw: int) -> int:
     """Max over DW-row tiles and channels of the tile's delay spread."""
-    d = np.atleast_2d(delays).astype(np.int64)
-    span = 0
-    for r0 in range(0, d.shape[0], dw):
-        blk = d[r0:r0 + dw]
-        span = max(span, int((blk.max(0) - blk.min(0)).max()))
-    return span
+    d = np.atleast_2d(delays)
+    ndm = d.shape[0]
+    pad = (-ndm) % dw
+    if pad:  # repeating the last row leaves the last tile's spread unchanged
+        d = np.concatenate([d, np.repeat(d[-1:], pad, axis=0)])
+    t = d.reshape(-1, dw, d.shape[1])
+    return int((t.max(axis=1).astype(np.int64) - t.min(axis=1)).max())
 
 
 class WorkList:
@@ -82,10 +83,12 @@ class WorkList:
     def add_job(self, *, planar_ptr: int, pitch_w: int, halo: int, nchans: int,
                 delays_dev: torch.Tensor, delays_host: np.ndarray, out_ptr: int, out_stride: int,
                 out_start: int, out_elem: int, nvalid: int, out_kind: int, sign: int = 1,
-                row_stride_out: int | None = None) -> None:
+                row_stride_out: int | None = None, span: int | None = None) -> None:
         """One DM-time job: rows of ``delays`` (ndm x >= nchans, row pitch =
         delays_dev.stride(0)) against ``nchans`` planar rows; output row r at
-        out_ptr + r * out_stride * out_elem."""
+        out_ptr + r * out_stride * out_elem.  ``span``: the job's tile span
+        (``tile_span`` of the signed delays for this variant's DW), when the
+        caller has it cached."""
         dh = np.atleast_2d(delays_host).astype(np.int64) * sign
         ndm = dh.shape[0]
         if delays_dev.dtype != torch.int32 or delays_dev.stride(-1) != 1:
@@ -94,7 +97,7 @@ class WorkList:
         T, DW = self.T, self.DW
         ntiles = max(1, -(-nvalid // T))
         dlo, dhi = int(dh[:, :nchans].min()), int(dh[:, :nchans].max())
-        self.span = max(self.span, tile_span(dh[:, :nchans], DW))
+        self.span = max(self.span, tile_span(dh[:, :nchans], DW) if span is None else int(span))
         r0 = np.arange(0, ndm, DW)
         nrows = np.minimum(DW, ndm - r0)
         t0 = np.arange(ntiles, dtype=np.int64) * T

@@ -93,10 +93,11 @@ static Variant mk(int single) {
 // Bit-sliced counters hold sums below 2^kBitLevels.
 constexpr int kBitLevels = 14;
 
-template <int NB, int P, int DW, int TW, int STAGES, int SLAB = 64, int SLOT = 0>
+template <int NB, int P, int DW, int TW, int STAGES, int SLAB = 64, int SLOT = 0, int MINB = 0>
 static Variant mkb() {
-  return Variant{NB, 0, P, DW, TW, SLAB, STAGES,
-                 &k_dmt_bits<NB, P, DW, TW, STAGES, kBitLevels, SLAB, SLOT>, 0, 1, SLOT};
+  void (*fn)(const DmtArgs) = &k_dmt_bits<NB, P, DW, TW, STAGES, kBitLevels, SLAB, SLOT>;
+  if constexpr (MINB > 0) fn = &k_dmt_bits_minb<NB, P, DW, TW, STAGES, kBitLevels, SLAB, SLOT, MINB>;
+  return Variant{NB, 0, P, DW, TW, SLAB, STAGES, fn, 0, 1, SLOT};
 }
 
 #define SPP_INT_VARIANTS(NB)                    \
@@ -106,9 +107,13 @@ static Variant mkb() {
 static const std::vector<Variant>& variants() {
   static const std::vector<Variant> v = {
       // bit-sliced (1- and 2-bit data)
+      // fixed slot widths first: 32-channel slabs keep 3-4 CTAs resident per SM
+      mkb<2, 2, 8, 1, 2, 32, 80, 4>(), mkb<2, 2, 8, 1, 2, 32, 80>(), mkb<2, 2, 8, 1, 3, 32, 80>(),
+      mkb<2, 2, 8, 1, 2, 32, 96>(), mkb<2, 2, 8, 1, 2, 32, 128>(),
       mkb<2, 2, 8, 1, 2, 64, 80>(), mkb<2, 2, 8, 1, 2, 64, 96>(),
       mkb<2, 2, 8, 1, 2>(), mkb<2, 2, 8, 1, 3, 32>(), mkb<2, 2, 8, 1, 2, 32>(),
       mkb<2, 4, 8, 1, 2, 32>(), mkb<2, 2, 16, 1, 2, 32>(), mkb<2, 1, 8, 1, 3>(),
+      mkb<1, 2, 8, 1, 2, 32, 80>(), mkb<1, 2, 8, 1, 2, 32, 128>(),
       mkb<1, 2, 8, 1, 2>(), mkb<1, 2, 8, 1, 3, 32>(), mkb<1, 4, 8, 1, 2, 32>(),
       SPP_INT_VARIANTS(1),
       SPP_INT_VARIANTS(2),

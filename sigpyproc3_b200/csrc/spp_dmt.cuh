@@ -930,9 +930,8 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
   }
 }
 
-template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT = 0>
-__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads)
-k_dmt_bits(const DmtArgs a) {
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT>
+__device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
   using Sh = BitsShape<NB, P, DW, TW, SLAB>;
   constexpr int NWC = Sh::kNwc;
   constexpr int T = Sh::kT;
@@ -1081,6 +1080,19 @@ k_dmt_bits(const DmtArgs a) {
         if (tb + i < a.nvalid) out[tb + i] = (float)cnt.count(p, i);
     }
   }
+}
+
+// The kernel without a minimum-residency hint (ptxas picks the register
+// count), and the same body with one (registers capped for MINB CTAs per SM).
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT = 0>
+__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads)
+k_dmt_bits(const DmtArgs a) {
+  dmt_bits_body<NB, P, DW, TW, STAGES, L, SLAB, SLOT>(a);
+}
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT, int MINB>
+__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads, MINB)
+k_dmt_bits_minb(const DmtArgs a) {
+  dmt_bits_body<NB, P, DW, TW, STAGES, L, SLAB, SLOT>(a);
 }
 
 // Corner turn into bit-plane rows (row c*NB + b: bit b of channel c, 32

@@ -74,6 +74,13 @@ class BeamState:
         self.hist = 0  # real stream rows held (right-aligned) in the tail, <= maxd
         self.next_seq = 0
         self.bitorder = _lib.BITORDER_LITTLE if h.nbits == 1 else _lib.BITORDER_BIG
+        self._spans: dict[int, int] = {}
+
+    def span(self, dw: int) -> int:
+        """Tile span of this beam's delay table for DM tiles of ``dw`` rows (cached)."""
+        if dw not in self._spans:
+            self._spans[dw] = tile_span(self.delays, dw)
+        return self._spans[dw]
 
 
 @dataclass
@@ -140,6 +147,16 @@ class Server:
             used += b
         return batch
 
+    def _group_key(self, st: BeamState) -> tuple[int, int]:
+        """Chunks of one sample width whose shared-memory slots are within a
+        factor 1.25 of each other share a work-list launch: each launch stages
+        slots as wide as its widest item, so mixing a wide-span beam with
+        narrow ones would copy (and hold) rows the narrow ones never read."""
+        cfg = variant_cfg(st.nbits, _lib.ACC_KAHAN32, self.variant)
+        slot = int(_lib.load().spp_wl_slot_words(st.nbits, _lib.ACC_KAHAN32, self.variant,
+                                                 st.span(cfg["DW"])))
+        return st.nbits, int(math.ceil(math.log(max(slot, 1)) / math.log(1.25)))
+
     def _launch(self, chunks: list[Chunk], now: float) -> None:
         stream = self.streams[self._rr % len(self.streams)]
         self._rr += 1
@@ -165,14 +182,14 @@ class Server:
             start_row = st.maxd - st.hist
             c.nvalid = st.hist + c.nsamps - st.maxd
             st.hist = min(st.maxd, st.hist + c.nsamps)
-            groups.setdefault(st.nbits, []).append((c, st, raw, start_row))
+            groups.setdefault(self._group_key(st), []).append((c, st, raw, start_row))
             total += self.chunk_bytes(c)
         stream.wait_stream(cs)
         wls = []
         with torch.cuda.stream(stream):
-            for nbits, items in groups.items():
+            for (nbits, _), items in groups.items():
                 wl = WorkList(nbits, self.variant, device=self.device)
-                span = max(tile_span(st.delays, wl.DW) for _, st, _, _ in items)
+                span = max(st.span(wl.DW) for _, st, _, _ in items)
                 slot = wl.slot_words(span)
                 for c, st, raw, start_row in items:
                     if c.nvalid <= 0:
@@ -187,7 +204,8 @@ class Server:
                     wl.add_job(planar_ptr=planar.data_ptr(), pitch_w=pitch, halo=halo,
                                nchans=st.nchans, delays_dev=st.delays_dev, delays_host=st.delays,
                                out_ptr=dmt.data_ptr(), out_stride=dmt.stride(0), out_start=0,
-                               out_elem=4, nvalid=c.nvalid, out_kind=_lib.OUT_I32)
+                               out_elem=4, nvalid=c.nvalid, out_kind=_lib.OUT_I32,
+                               span=st.span(wl.DW))
                     bufs += [raw, planar, dmt]
                     c.dmt = dmt
                 if wl._rows:
