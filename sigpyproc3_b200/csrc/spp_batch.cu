@@ -12,17 +12,20 @@ struct WlVariant {
   int nb, acc, R, DW, TW, SLAB, STAGES;
   void (*fn)(const WlArgs);
   int planes;  // 1: bit-sliced over bit-plane rows (R = words per thread)
+  int slot;    // > 0: kernel compiled for exactly this slot width (words)
 };
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
 static WlVariant mkwl() {
-  return WlVariant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt_wl<NB, R, DW, TW, SLAB, STAGES, ACC>, 0};
+  return WlVariant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt_wl<NB, R, DW, TW, SLAB, STAGES, ACC>, 0,
+                   0};
 }
 
-template <int NB, int P, int DW, int TW, int STAGES, int SLAB>
+template <int NB, int P, int DW, int TW, int STAGES, int SLAB, int SLOT = 0, int MINB = 0>
 static WlVariant mkwlb() {
-  return WlVariant{NB, 0, P, DW, TW, SLAB, STAGES,
-                   &k_dmt_bits_wl<NB, P, DW, TW, STAGES, 14, SLAB>, 1};
+  void (*fn)(const WlArgs) = &k_dmt_bits_wl<NB, P, DW, TW, STAGES, 14, SLAB, SLOT>;
+  if constexpr (MINB > 0) fn = &k_dmt_bits_wl_minb<NB, P, DW, TW, STAGES, 14, SLAB, SLOT, MINB>;
+  return WlVariant{NB, 0, P, DW, TW, SLAB, STAGES, fn, 1, SLOT};
 }
 
 #define SPP_WL_INT(NB)                                                                  \
@@ -31,7 +34,10 @@ static WlVariant mkwlb() {
 
 static const std::vector<WlVariant>& wl_variants() {
   static const std::vector<WlVariant> v = {
+      // fixed slot widths first (4 CTAs per SM), then runtime widths
+      mkwlb<1, 2, 8, 1, 2, 32, 80, 4>(), mkwlb<1, 2, 8, 1, 2, 32, 128, 4>(),
       mkwlb<1, 2, 8, 1, 2, 64>(), mkwlb<1, 2, 8, 1, 3, 32>(),
+      mkwlb<2, 2, 8, 1, 2, 32, 80, 4>(), mkwlb<2, 2, 8, 1, 2, 32, 128, 4>(),
       mkwlb<2, 2, 8, 1, 2, 64>(), mkwlb<2, 2, 8, 1, 3, 32>(),
       SPP_WL_INT(1), SPP_WL_INT(2), SPP_WL_INT(4), SPP_WL_INT(8), SPP_WL_INT(16),
       mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_KAHAN32>(), mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_KAHAN32>(),
@@ -58,7 +64,9 @@ static int64_t wl_T(const WlVariant& v) { return (int64_t)v.TW * 32 * v.R * spw_
 static int32_t wl_slot(const WlVariant& v, int32_t span) {
   const int spw = spw_wl(v);
   const int64_t w = wl_T(v) / spw + ceil_div(std::max<int32_t>(span, 0), spw) + 6 + v.R;
-  return (int32_t)round_up(w, 4);
+  const int32_t need = (int32_t)round_up(w, 4);
+  if (v.slot > 0) return need <= v.slot ? v.slot : -1;  // fixed-width kernels
+  return need;
 }
 
 static int64_t wl_smem(const WlVariant& v, int32_t slot_w) {
@@ -111,6 +119,9 @@ int spp_wl_launch(int nbits, int acc, int variant, const void* items, int32_t ni
   if (!v) return fail(SPP_ERR_ARG, "no work-list variant %d for nbits=%d acc=%d", variant, nbits, acc);
   if (!items || !counter || nitems < 0 || slot_w <= 0 || (slot_w & 3))
     return fail(SPP_ERR_ARG, "bad work-list arguments");
+  if (v->slot > 0 && slot_w != v->slot)
+    return fail(SPP_ERR_ARG, "work-list variant %d takes slot width %d (got %d)", variant, v->slot,
+                slot_w);
   if (nitems == 0) return SPP_OK;
   const int64_t smem = wl_smem(*v, slot_w);
   if (smem > 227 * 1024) return fail(SPP_ERR_UNSUPPORTED, "work list needs %lld B shared memory", (long long)smem);

@@ -1164,9 +1164,8 @@ k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t ns
 // Persistent work-list version of the bit-sliced kernel (same items as
 // k_dmt_wl; planar rows are bit-plane rows, NB per channel).
 // ----------------------------------------------------------------------------
-template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB>
-__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads)
-k_dmt_bits_wl(const WlArgs w) {
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT>
+__device__ __forceinline__ void dmt_bits_wl_body(const WlArgs& w) {
   using Sh = BitsShape<NB, P, DW, TW, SLAB>;
   constexpr int NWC = Sh::kNwc;
   constexpr int JJ = (SLAB + 31) / 32;
@@ -1300,8 +1299,8 @@ k_dmt_bits_wl(const WlArgs w) {
     const int nc = min(SLAB, it.nchans - k * SLAB);
     const uint32_t* sd = sdata + (int64_t)s * SLAB * NB * w.slot_w;
     const int32_t* off = soff + (s * DW + dmw) * SLAB;
-    if (nc == SLAB) bits_slab<NB, P, L, SLAB, true>(cnt, sd, off, nc, w.slot_w, wbase);
-    else bits_slab<NB, P, L, SLAB, false>(cnt, sd, off, nc, w.slot_w, wbase);
+    if (nc == SLAB) bits_slab<NB, P, L, SLAB, true, SLOT>(cnt, sd, off, nc, w.slot_w, wbase);
+    else bits_slab<NB, P, L, SLAB, false, SLOT>(cnt, sd, off, nc, w.slot_w, wbase);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     if (k == nslab - 1 && dmw < it.nrows) {
@@ -1327,5 +1326,18 @@ k_dmt_bits_wl(const WlArgs w) {
       }
     }
   }
+}
+
+// Work-list kernel without / with a minimum-residency hint (SLOT > 0: the
+// launch's slot width must equal SLOT).
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT = 0>
+__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads)
+k_dmt_bits_wl(const WlArgs w) {
+  dmt_bits_wl_body<NB, P, DW, TW, STAGES, L, SLAB, SLOT>(w);
+}
+template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT, int MINB>
+__global__ void __launch_bounds__(BitsShape<NB, P, DW, TW, SLAB>::kThreads, MINB)
+k_dmt_bits_wl_minb(const WlArgs w) {
+  dmt_bits_wl_body<NB, P, DW, TW, STAGES, L, SLAB, SLOT>(w);
 }
 }  // namespace spp

@@ -75,6 +75,7 @@ class BeamState:
         self.next_seq = 0
         self.bitorder = _lib.BITORDER_LITTLE if h.nbits == 1 else _lib.BITORDER_BIG
         self._spans: dict[int, int] = {}
+        self.pick: tuple[int, int] | None = None  # (work-list variant, slot width)
 
     def span(self, dw: int) -> int:
         """Tile span of this beam's delay table for DM tiles of ``dw`` rows (cached)."""
@@ -96,7 +97,7 @@ class _Batch:
 class Server:
     def __init__(self, beams: list[BeamSpec], *, hbm_budget: int = 40 << 30,
                  widths=(1, 2, 4, 8, 16, 32, 64, 128), max_inflight: int = 2,
-                 keep_dmt: bool = False, variant: int = 0, device=None):
+                 keep_dmt: bool = False, variant: int | None = None, device=None):
         self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
         self.beams = {b.beam_id: BeamState(b, self.device) for b in beams}
         self.budget = int(hbm_budget)
@@ -114,10 +115,30 @@ class Server:
         self.batches = 0
 
     # ---- sizing ----
+    def _pick(self, st: BeamState) -> tuple[int, int]:
+        """Work-list kernel for a beam: ``variant`` if given, else the first
+        variant (fixed-slot kernels come first) whose shared-memory slot holds
+        the beam's tile span within the per-CTA limit.  Returns (variant, slot)."""
+        if st.pick is None:
+            lib = _lib.load()
+            acc = _lib.ACC_KAHAN32
+            cands = [self.variant] if self.variant is not None else \
+                range(lib.spp_wl_num_variants(st.nbits, acc))
+            for v in cands:
+                dw = variant_cfg(st.nbits, acc, v)["DW"]
+                slot = int(lib.spp_wl_slot_words(st.nbits, acc, v, st.span(dw)))
+                if slot > 0 and lib.spp_wl_smem_bytes(st.nbits, acc, v, slot) <= 227 * 1024:
+                    st.pick = (v, slot)
+                    break
+            else:
+                raise ValueError(f"beam {st.spec.beam_id}: no work-list kernel holds its delay "
+                                 "spread")
+        return st.pick
+
     def chunk_bytes(self, c: Chunk) -> int:
         st = self.beams[c.beam_id]
         rows = c.nsamps + st.maxd
-        cfg = variant_cfg(st.nbits, _lib.ACC_KAHAN32, self.variant)
+        cfg = variant_cfg(st.nbits, _lib.ACC_KAHAN32, self._pick(st)[0])
         spw = cfg["spw"]
         planes = st.nbits if cfg["planes"] else 1
         planar = st.nchans * planes * (rows // spw + 4096) * 4
@@ -147,15 +168,14 @@ class Server:
             used += b
         return batch
 
-    def _group_key(self, st: BeamState) -> tuple[int, int]:
-        """Chunks of one sample width whose shared-memory slots are within a
-        factor 1.25 of each other share a work-list launch: each launch stages
-        slots as wide as its widest item, so mixing a wide-span beam with
-        narrow ones would copy (and hold) rows the narrow ones never read."""
-        cfg = variant_cfg(st.nbits, _lib.ACC_KAHAN32, self.variant)
-        slot = int(_lib.load().spp_wl_slot_words(st.nbits, _lib.ACC_KAHAN32, self.variant,
-                                                 st.span(cfg["DW"])))
-        return st.nbits, int(math.ceil(math.log(max(slot, 1)) / math.log(1.25)))
+    def _group_key(self, st: BeamState) -> tuple[int, int, int]:
+        """Chunks of one sample width and kernel whose shared-memory slots are
+        within a factor 1.25 of each other share a work-list launch: each
+        launch stages slots as wide as its widest item, so mixing a wide-span
+        beam with narrow ones would copy (and hold) rows the narrow ones never
+        read."""
+        v, slot = self._pick(st)
+        return st.nbits, v, int(math.ceil(math.log(max(slot, 1)) / math.log(1.25)))
 
     def _launch(self, chunks: list[Chunk], now: float) -> None:
         stream = self.streams[self._rr % len(self.streams)]
@@ -187,8 +207,8 @@ class Server:
         stream.wait_stream(cs)
         wls = []
         with torch.cuda.stream(stream):
-            for (nbits, _), items in groups.items():
-                wl = WorkList(nbits, self.variant, device=self.device)
+            for (nbits, v, _), items in groups.items():
+                wl = WorkList(nbits, v, device=self.device)
                 span = max(st.span(wl.DW) for _, st, _, _ in items)
                 slot = wl.slot_words(span)
                 for c, st, raw, start_row in items:
