@@ -95,6 +95,20 @@ int spp_dedisperse(const void* in, int nbits, int bitorder, int64_t nchans,
                    int64_t out_start, int acc, void* workspace,
                    int64_t workspace_bytes, void* stream);
 
+/* The same computation for 8-bit data with `delays_host` in HOST memory -- the
+ * form kernels.dedisperse(in, out, delays, nchans, nsamps, out_start) takes it
+ * (core/kernels.py:340-347).  Knowing the delays on the host lets the call
+ * precompute every row range and channel offset into the kernel's parameters
+ * (one launch, no workspace, no delay upload; a CUDA graph that captures the
+ * call records the parameters).  Returns SPP_ERR_UNSUPPORTED (nothing
+ * launched) unless
+ * nbits == 8, nchans is a multiple of 32 and at most 1024, `in` is 16-B
+ * aligned and the block's slabs fit in shared memory together; callers then
+ * use spp_dedisperse. */
+int spp_dedisperse_hd(const void* in, int nbits, int64_t nchans, int64_t nsamps,
+                      const int32_t* delays_host, float* out, int64_t out_len,
+                      int64_t out_start, void* stream);
+
 /* Same computation as spp_dedisperse, but allocating nothing and taking no
  * workspace.  No counterpart in the reference.  It serves callers that must not
  * allocate device memory while running (a real-time pipeline that reserves its

@@ -17,6 +17,8 @@ namespace spp {
 int launch_single8(const uint8_t* raw, int64_t nchans, int64_t nsamps, const int32_t* delays,
                    int32_t dlo, int32_t dhi, float* out, int64_t out_start, int64_t nvalid,
                    uint32_t* status, cudaStream_t st);
+int launch_single8_hd(const uint8_t* raw, int64_t nchans, int64_t nsamps, const int32_t* delays_host,
+                      float* out, int64_t out_start, int64_t nvalid, cudaStream_t st);
 
 static thread_local char g_err[1024] = "";
 
@@ -396,6 +398,30 @@ int spp_dedisperse(const void* in, int nbits, int bitorder, int64_t nchans, int6
   a.nvalid = g.nvalid;
   a.status = reinterpret_cast<uint32_t*>(ws);
   return launch_dmt(*v, a, g.ntiles_t, 1, st);
+}
+
+int spp_dedisperse_hd(const void* in, int nbits, int64_t nchans, int64_t nsamps,
+                      const int32_t* delays_host, float* out, int64_t out_len, int64_t out_start,
+                      void* stream) {
+  if (!in || !delays_host || !out) return fail(SPP_ERR_ARG, "spp_dedisperse_hd: null pointer");
+  if (nbits != 8) return fail(SPP_ERR_UNSUPPORTED, "host-table path covers 8-bit data");
+  if (nchans <= 0 || nsamps <= 0) return fail(SPP_ERR_ARG, "bad shape");
+  const int32_t dmin = *std::min_element(delays_host, delays_host + nchans);
+  const int32_t dmax = *std::max_element(delays_host, delays_host + nchans);
+  const int64_t maxabs = std::max<int64_t>(std::llabs(dmin), std::llabs(dmax));
+  const int64_t nvalid = nsamps - maxabs;
+  if (nvalid <= 0) return SPP_OK;  // reference: prange over a non-positive count
+  if (-(int64_t)dmin > nsamps)
+    return fail(SPP_ERR_DELAY, "negative delay %d reaches before the block", dmin);
+  if (out_start < 0 || out_start + nvalid > out_len)
+    return fail(SPP_ERR_SIZE, "output too small: out_start %lld + %lld samples > out_len %lld",
+                (long long)out_start, (long long)nvalid, (long long)out_len);
+  const int rc = launch_single8_hd(static_cast<const uint8_t*>(in), nchans, nsamps, delays_host,
+                                   out, out_start, nvalid, as_stream(stream));
+  if (rc == SPP_ERR_UNSUPPORTED)
+    return fail(rc, "host-table path needs nchans %% 32 == 0, nchans <= 1024, a 16-B aligned "
+                "block and every slab resident in shared memory");
+  return rc;
 }
 
 }  // extern "C"

@@ -70,12 +70,15 @@ def dedisperse_block(raw: torch.Tensor, delays: np.ndarray, nchans: int, nsamps:
                      bitorder: str = "big", acc: int = _lib.ACC_F64,
                      delays_dev: torch.Tensor | None = None,
                      stream: torch.cuda.Stream | None = None,
-                     ws: torch.Tensor | None = None) -> int:
+                     ws: torch.Tensor | None = None, host_table: bool | None = None) -> int:
     """``out[out_start + t] = sum_c x[t + delays[c]][c]`` for ``t < nsamps - max|d|``.
 
     Returns the number of samples written.  ``raw`` holds ``nsamps`` spectra
     (uint8 packed or float32).  ``delays`` is the host int32 table (its range
     bounds the kernel's checks); ``delays_dev`` may carry a device copy.
+    8-bit blocks go through ``spp_dedisperse_hd`` (offsets precomputed from the
+    host table) when their shape allows, else through ``spp_dedisperse``;
+    ``host_table`` True/False forces one of the two.
     """
     raw = _as_raw(raw)
     nb = _nbits_of(raw, nbits)
@@ -88,8 +91,6 @@ def dedisperse_block(raw: torch.Tensor, delays: np.ndarray, nchans: int, nsamps:
         return 0
     if out.dtype != torch.float32 or not out.is_cuda:
         raise TypeError("out must be a CUDA float32 tensor")
-    if delays_dev is None:
-        delays_dev = torch.from_numpy(delays).to(raw.device, non_blocking=False)
     lib = _lib.load()
     need = lib.spp_dedisperse_workspace_bytes(nb, nchans, nsamps, dmin, dmax)
     if need < 0:
@@ -97,6 +98,17 @@ def dedisperse_block(raw: torch.Tensor, delays: np.ndarray, nchans: int, nsamps:
     if ws is None:
         ws = workspace(need, raw.device, stream)
     st = stream_handle(stream, raw.device)
+    if nb == 8 and host_table is not False:
+        rc = lib.spp_dedisperse_hd(raw.data_ptr(), nb, nchans, nsamps, delays.ctypes.data,
+                                   out.data_ptr(), out.numel(), out_start, st)
+        if rc == _lib.SPP_OK:
+            return nvalid
+        if rc != _lib.SPP_ERR_UNSUPPORTED or host_table:
+            _lib.check(rc)
+    elif host_table:
+        raise NotImplementedError("the host-table path covers 8-bit data")
+    if delays_dev is None:
+        delays_dev = torch.from_numpy(delays).to(raw.device, non_blocking=False)
     _lib.check(lib.spp_dedisperse(
         raw.data_ptr(), nb, bitorder_code(bitorder), nchans, nsamps, delays_dev.data_ptr(),
         dmin, dmax, out.data_ptr(), out.numel(), out_start, acc, ws.data_ptr(), ws.numel(), st))
