@@ -72,6 +72,25 @@ def run_c1(args, rank, world, local, emit) -> None:
     e3.record()
     e3.synchronize()
     ms_eager = e2.elapsed_time(e3) / (nrot * 4)
+    # context, not the product: a plain device-to-device copy of each 17 MB
+    # input (torch copy_, 2x the bytes this call reads), same rotation and replay
+    dsts = [torch.empty_like(r) for r in raws]
+    cg = torch.cuda.CUDAGraph()
+    cs.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.graph(cg, stream=cs):
+        for i in range(nrot):
+            dsts[i].copy_(raws[i])
+    torch.cuda.current_stream().wait_stream(cs)
+    for _ in range(3):
+        cg.replay()
+    e4, e5 = _events()
+    e4.record()
+    for _ in range(reps):
+        cg.replay()
+    e5.record()
+    e5.synchronize()
+    copy_us = e4.elapsed_time(e5) * 1e3 / (reps * nrot)
+    del dsts, cg
     alg = g.nsamps * g.nchans + nv * 4
     peaks = json.loads((Path(__file__).resolve().parents[1] / "MEASURED_PEAKS.json").read_text()) \
         if (Path(__file__).resolve().parents[1] / "MEASURED_PEAKS.json").exists() else {"hbm_gbs": 6650.0}
@@ -85,7 +104,11 @@ def run_c1(args, rank, world, local, emit) -> None:
                      "input copies (L2-cold)"},
              roofline={"bound": "hbm", "achieved": gbs, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                        "frac": gbs / peaks["hbm_gbs"], "algorithmic_bytes": alg,
-                       "note": "single-pass 8-bit kernel, one launch per call, CUDA-graph replay"},
+                       "note": "single-pass 8-bit kernel (spp_dedisperse_hd), one launch per "
+                               "call, CUDA-graph replay"},
+             reference_copy={"us_per_call": copy_us, "bytes_moved": 2 * g.nsamps * g.nchans,
+                             "note": "torch copy_ of the same 17 MB input, same replay: what one "
+                                     "launch moving these bytes costs at this size"},
              eager_ms_per_call=ms_eager, pulse_at=int(np.argmax(ref)))
 
 
