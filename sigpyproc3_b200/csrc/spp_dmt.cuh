@@ -854,16 +854,17 @@ struct BitsShape {
 };
 
 // Shared memory per stage: SLAB channels x NB plane rows x slot_w words, plus
-// DW x SLAB tile-relative sample offsets.
+// DW x SLAB tile-relative sample offsets, each stored decoded as (word, bit
+// shift) so the consumers spend no instructions splitting it.
 __host__ __device__ constexpr int64_t bits_stage_bytes(int nb, int slab, int slot_w, int dw) {
-  return (int64_t)slab * nb * slot_w * 4 + (int64_t)dw * slab * 4;
+  return (int64_t)slab * nb * slot_w * 4 + (int64_t)dw * slab * 8;
 }
 
 // One slab of SLAB channels through the carry-save network.  FULL: all
 // channels present (no predicates); otherwise channels >= nc add zeros.
 template <int NB, int P, int L, int SLAB, bool FULL, int SLOT = 0>
 __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t* __restrict__ sd,
-                                          const int32_t* __restrict__ off, int nc, int slot_rt,
+                                          const int2* __restrict__ off, int nc, int slot_rt,
                                           int wbase) {
   // SLOT > 0: slot width known at compile time (immediate load offsets)
   const int slot_w = SLOT > 0 ? SLOT : slot_rt;
@@ -879,9 +880,9 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
       for (int q = 0; q < 4; ++q) {
         const int j = 16 * m + 4 * i + q;
         const bool live = FULL || j < nc;
-        const int o = live ? off[j] : 0;
-        const int sh = o & 31;
-        const uint32_t* base = sd + j * NB * slot_w + (o >> 5) + wbase;
+        const int2 ow = live ? off[j] : make_int2(0, 0);  // (word, bit shift)
+        const int sh = ow.y;
+        const uint32_t* base = sd + j * NB * slot_w + ow.x + wbase;
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
 #pragma unroll
@@ -940,7 +941,7 @@ __device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
 
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
-  int32_t* soff = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * NB * a.slot_w);
+  int2* soff = reinterpret_cast<int2*>(sdata + (int64_t)STAGES * SLAB * NB * a.slot_w);
   uint64_t* full = reinterpret_cast<uint64_t*>(soff + STAGES * DW * SLAB);
   uint64_t* empty = full + STAGES;
 
@@ -1005,8 +1006,10 @@ __device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
           const int64_t ws = ((t0 + mn[jj] + a.halo) / 32) & ~int64_t(3);
           const int32_t base = (int32_t)(ws * 32 - a.halo - t0);
 #pragma unroll
-          for (int i = 0; i < DW; ++i)
-            soff[(s * DW + i) * SLAB + j] = min(dv[jj][i], mx[jj]) - base;
+          for (int i = 0; i < DW; ++i) {
+            const int32_t o = min(dv[jj][i], mx[jj]) - base;  // >= 0: base <= min delay
+            soff[(s * DW + i) * SLAB + j] = make_int2(o >> 5, o & 31);
+          }
           ws_reg[jj] = ws;
         }
       }
@@ -1040,7 +1043,7 @@ __device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
     if (!mbar_wait(&full[s], (k / STAGES) & 1, a.status)) { ok = false; break; }
     const int nc = min(SLAB, a.nchans - k * SLAB);
     const uint32_t* sd = sdata + (int64_t)s * SLAB * NB * a.slot_w;
-    const int32_t* off = soff + (s * DW + dmw) * SLAB;
+    const int2* off = soff + (s * DW + dmw) * SLAB;
     if (nc == SLAB) bits_slab<NB, P, L, SLAB, true, SLOT>(cnt, sd, off, nc, a.slot_w, wbase);
     else bits_slab<NB, P, L, SLAB, false, SLOT>(cnt, sd, off, nc, a.slot_w, wbase);
     __syncwarp();
@@ -1172,8 +1175,8 @@ __device__ __forceinline__ void dmt_bits_wl_body(const WlArgs& w) {
 
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
-  int32_t* soff = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * NB * w.slot_w);
-  int32_t* stag = soff + STAGES * DW * SLAB;  // per stage: item, slab, nslab, pad
+  int2* soff = reinterpret_cast<int2*>(sdata + (int64_t)STAGES * SLAB * NB * w.slot_w);
+  int32_t* stag = reinterpret_cast<int32_t*>(soff + STAGES * DW * SLAB);  // per stage: item, slab, nslab, pad
   uint64_t* full = reinterpret_cast<uint64_t*>(stag + 4 * STAGES);
   uint64_t* empty = full + STAGES;
 
@@ -1243,8 +1246,10 @@ __device__ __forceinline__ void dmt_bits_wl_body(const WlArgs& w) {
             const int64_t ws = ((it.t0 + mn[jj] + it.halo) / 32) & ~int64_t(3);
             const int32_t base = (int32_t)(ws * 32 - it.halo - it.t0);
 #pragma unroll
-            for (int i = 0; i < DW; ++i)
-              soff[(s * DW + i) * SLAB + j] = min(dv[jj][i], mx[jj]) - base;
+            for (int i = 0; i < DW; ++i) {
+              const int32_t o = min(dv[jj][i], mx[jj]) - base;  // >= 0: base <= min delay
+              soff[(s * DW + i) * SLAB + j] = make_int2(o >> 5, o & 31);
+            }
             ws_reg[jj] = ws;
           }
         }
@@ -1298,7 +1303,7 @@ __device__ __forceinline__ void dmt_bits_wl_body(const WlArgs& w) {
     }
     const int nc = min(SLAB, it.nchans - k * SLAB);
     const uint32_t* sd = sdata + (int64_t)s * SLAB * NB * w.slot_w;
-    const int32_t* off = soff + (s * DW + dmw) * SLAB;
+    const int2* off = soff + (s * DW + dmw) * SLAB;
     if (nc == SLAB) bits_slab<NB, P, L, SLAB, true, SLOT>(cnt, sd, off, nc, w.slot_w, wbase);
     else bits_slab<NB, P, L, SLAB, false, SLOT>(cnt, sd, off, nc, w.slot_w, wbase);
     __syncwarp();
