@@ -126,11 +126,15 @@ def test_dedisperse_block_edge_cases(torch_cuda, orc):
 
 
 @pytest.mark.parametrize("nbits", [1, 2, 4, 8])
-def test_dmt_plan_all_variants(torch_cuda, orc, nbits):
+@pytest.mark.parametrize("wide", [True, False])
+def test_dmt_plan_all_variants(torch_cuda, orc, nbits, wide):
+    """Every kernel variant; 136/128 channels (5 or 4 slabs of 32, the last
+    partial) and 96 channels (3 full slabs: an odd slab count)."""
     torch = torch_cuda
     from sigpyproc3_b200.dedisp import DMTPlan
 
-    nchans, nsamps, ndm = 136 if nbits != 1 else 128, 2500, 19
+    nchans = (136 if nbits != 1 else 128) if wide else 96
+    nsamps, ndm = 2500, 19
     rng = np.random.default_rng(7 + nbits)
     vals = rng.integers(0, 1 << nbits, size=nsamps * nchans, dtype=np.uint8)
     raw = vals if nbits == 8 else _pack(vals, nbits, "big")
