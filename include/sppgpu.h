@@ -56,7 +56,8 @@ extern "C" {
 #define SPP_MODE_ROLL 1       /* out[t] = sum_c x[(t - d_c) mod n][c] (kernels.dmt_block) */
 
 /* float accumulation for float32 input */
-#define SPP_ACC_KAHAN32 0 /* compensated fp32 (Kahan 1965)                       */
+#define SPP_ACC_KAHAN32 0 /* fp32 partial per slab of <= 32 channels, compensated
+                             (Kahan 1965) sum across slabs                      */
 #define SPP_ACC_F64 1     /* fp64 accumulator, as the reference kernels          */
 
 const char* spp_last_error_string(void);

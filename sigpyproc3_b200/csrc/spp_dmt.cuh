@@ -391,20 +391,28 @@ k_dmt(const DmtArgs a) {
       const float* sd = reinterpret_cast<const float*>(sdata) + (int64_t)s * SLAB * a.slot_w;
       const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
       const int32_t* bs = sbase + s * SLAB;
+      // SPP_ACC_KAHAN32: a plain fp32 partial over the slab (<= 32 channels),
+      // then one compensated (Kahan) step per slab into the running sum
+      float p_acc[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) p_acc[r] = 0.f;
 #pragma unroll 4
       for (int j = 0; j < nc; ++j) {
         const float* row = sd + j * a.slot_w + (wbase + dl[j] - bs[j]);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const float x = row[32 * r];
-          if (ACC == SPP_ACC_F64) {
-            d_acc[r] += (double)x;
-          } else {
-            const float y = __fsub_rn(x, c_acc[r]);
-            const float t = __fadd_rn(s_acc[r], y);
-            c_acc[r] = __fsub_rn(__fsub_rn(t, s_acc[r]), y);
-            s_acc[r] = t;
-          }
+          if (ACC == SPP_ACC_F64) d_acc[r] += (double)x;
+          else p_acc[r] = __fadd_rn(p_acc[r], x);
+        }
+      }
+      if (ACC != SPP_ACC_F64) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float y = __fsub_rn(p_acc[r], c_acc[r]);
+          const float t = __fadd_rn(s_acc[r], y);
+          c_acc[r] = __fsub_rn(__fsub_rn(t, s_acc[r]), y);
+          s_acc[r] = t;
         }
       }
       __syncwarp();
@@ -686,20 +694,28 @@ k_dmt_wl(const WlArgs w) {
       const float* sd = reinterpret_cast<const float*>(sdata) + (int64_t)s * SLAB * w.slot_w;
       const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
       const int32_t* bs = sbase + s * SLAB;
+      // SPP_ACC_KAHAN32: a plain fp32 partial over the slab (<= 32 channels),
+      // then one compensated (Kahan) step per slab into the running sum
+      float p_acc[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) p_acc[r] = 0.f;
 #pragma unroll 4
       for (int j = 0; j < nc; ++j) {
         const float* row = sd + j * w.slot_w + (wbase + dl[j] - bs[j]);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const float x = row[32 * r];
-          if (ACC == SPP_ACC_F64) {
-            d_acc[r] += (double)x;
-          } else {
-            const float y = __fsub_rn(x, c_acc[r]);
-            const float t = __fadd_rn(s_acc[r], y);
-            c_acc[r] = __fsub_rn(__fsub_rn(t, s_acc[r]), y);
-            s_acc[r] = t;
-          }
+          if (ACC == SPP_ACC_F64) d_acc[r] += (double)x;
+          else p_acc[r] = __fadd_rn(p_acc[r], x);
+        }
+      }
+      if (ACC != SPP_ACC_F64) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float y = __fsub_rn(p_acc[r], c_acc[r]);
+          const float t = __fadd_rn(s_acc[r], y);
+          c_acc[r] = __fsub_rn(__fsub_rn(t, s_acc[r]), y);
+          s_acc[r] = t;
         }
       }
       __syncwarp();

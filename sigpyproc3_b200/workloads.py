@@ -208,7 +208,8 @@ def run_c5(args, rank, world, local, emit) -> None:
     g = synth.C5
     nsamps = args.nsamps or g.nsamps
     ndm = args.ndm or 4096
-    dms = synth.dm_grid(1500.0, 4096)[np.linspace(0, 4095, ndm).astype(int)]
+    lo = (4096 - ndm) // 2  # profiling cases: a contiguous block of the full grid's trials
+    dms = synth.dm_grid(1500.0, 4096)[lo:lo + ndm]
     d = np.atleast_2d(g.delays(dms)).astype(np.int32)
     x = synth.gauss_f32_device(nsamps * g.nchans, 5)
     h = Header(nchans=g.nchans, fch1=g.fch1, foff=g.foff, tsamp=g.tsamp, nbits=32,
@@ -216,8 +217,9 @@ def run_c5(args, rank, world, local, emit) -> None:
     nv = nsamps - int(d.max())
     out = torch.empty((ndm, nv), dtype=torch.float32, device="cuda")
     # pick the accumulator and tile shape by timing one transform of each
+    # (--variant fixes a compensated-fp32 variant instead, for profiling)
     tune = []
-    for acc in (_lib.ACC_KAHAN32, _lib.ACC_F64):
+    for acc in (_lib.ACC_KAHAN32, _lib.ACC_F64) if args.variant is None else ():
         p = DMTPlan(d, g.nchans, nsamps, nbits=32, acc=acc)
         for v in range(p.num_variants):
             p.set_variant(v)
@@ -229,7 +231,7 @@ def run_c5(args, rank, world, local, emit) -> None:
             e1.synchronize()
             tune.append((e0.elapsed_time(e1), acc, v))
         p.close()
-    best = min(tune)
+    best = min(tune) if tune else (0.0, _lib.ACC_KAHAN32, args.variant)
     plan = DMTPlan(d, g.nchans, nsamps, nbits=32, acc=best[1])
     plan.set_variant(best[2])
     widths = tuple(1 << k for k in range(10))
