@@ -295,7 +295,7 @@ k_dmt(const DmtArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
   int32_t* sdel = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * a.slot_w);
-  int32_t* sbase = sdel + STAGES * DW * SLAB;
+  int32_t* sbase = sdel + STAGES * DW * SLAB;  // reserved: window starts are folded into sdel
   uint64_t* full = reinterpret_cast<uint64_t*>(sbase + STAGES * SLAB + ((STAGES * SLAB) & 1));
   uint64_t* empty = full + STAGES;
 
@@ -347,11 +347,11 @@ k_dmt(const DmtArgs a) {
             dev_flag(a.status, SPP_DEV_RANGE, (uint32_t)c | 0x80000000u);
             mx = mn + a.span_max;
           }
-#pragma unroll
-          for (int i = 0; i < DW; ++i)
-            sdel[(s * DW + i) * SLAB + j] = min(dv[i], mx);
+          // each trial's sample offset from the start of the staged window
           const int64_t ws = ((t0 + mn + a.halo) / SPW) & ~int64_t(3);
-          sbase[s * SLAB + j] = (int32_t)(ws * SPW - a.halo - t0);
+          const int32_t base = (int32_t)(ws * SPW - a.halo - t0);
+#pragma unroll
+          for (int i = 0; i < DW; ++i) sdel[(s * DW + i) * SLAB + j] = min(dv[i], mx) - base;
           ws_reg[jj] = ws;
         }
       }
@@ -390,7 +390,6 @@ k_dmt(const DmtArgs a) {
       const int nc = min(SLAB, a.nchans - k * SLAB);
       const float* sd = reinterpret_cast<const float*>(sdata) + (int64_t)s * SLAB * a.slot_w;
       const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
-      const int32_t* bs = sbase + s * SLAB;
       // SPP_ACC_KAHAN32: a plain fp32 partial over the slab (<= 32 channels),
       // then one compensated (Kahan) step per slab into the running sum
       float p_acc[R];
@@ -398,7 +397,7 @@ k_dmt(const DmtArgs a) {
       for (int r = 0; r < R; ++r) p_acc[r] = 0.f;
 #pragma unroll 4
       for (int j = 0; j < nc; ++j) {
-        const float* row = sd + j * a.slot_w + (wbase + dl[j] - bs[j]);
+        const float* row = sd + j * a.slot_w + (wbase + dl[j]);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const float x = row[32 * r];
@@ -439,12 +438,11 @@ k_dmt(const DmtArgs a) {
       const int nc = min(SLAB, a.nchans - k * SLAB);
       const uint32_t* sd = sdata + (int64_t)s * SLAB * a.slot_w;
       const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
-      const int32_t* bs = sbase + s * SLAB;
       for (int jb = 0; jb < nc; jb += F8) {
         const int je = min(nc, jb + F8);
 #pragma unroll 4
         for (int j = jb; j < je; ++j) {
-          const int o = dl[j] - bs[j];  // sample offset of the tile start in the slot
+          const int o = dl[j];  // sample offset of the tile start in the slot
           const uint32_t* row = sd + j * a.slot_w + (o >> P::kLogSpw) + wbase;
           const int sh = (o & (SPW - 1)) * NB;
 #pragma unroll
@@ -573,7 +571,7 @@ k_dmt_wl(const WlArgs w) {
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
   int32_t* sdel = reinterpret_cast<int32_t*>(sdata + (int64_t)STAGES * SLAB * w.slot_w);
-  int32_t* sbase = sdel + STAGES * DW * SLAB;
+  int32_t* sbase = sdel + STAGES * DW * SLAB;  // reserved: window starts are folded into sdel
   int32_t* stag = sbase + STAGES * SLAB;  // per stage: item, slab, nslab, pad
   uint64_t* full = reinterpret_cast<uint64_t*>(stag + 4 * STAGES);
   uint64_t* empty = full + STAGES;
@@ -634,10 +632,11 @@ k_dmt_wl(const WlArgs w) {
               dev_flag(w.status, SPP_DEV_RANGE, (uint32_t)c | 0x80000000u);
               mx = mn + it.span_max;
             }
-#pragma unroll
-            for (int i = 0; i < DW; ++i) sdel[(s * DW + i) * SLAB + j] = min(dv[i], mx);
+            // each trial's sample offset from the start of the staged window
             const int64_t ws = ((it.t0 + mn + it.halo) / SPW) & ~int64_t(3);
-            sbase[s * SLAB + j] = (int32_t)(ws * SPW - it.halo - it.t0);
+            const int32_t base = (int32_t)(ws * SPW - it.halo - it.t0);
+#pragma unroll
+            for (int i = 0; i < DW; ++i) sdel[(s * DW + i) * SLAB + j] = min(dv[i], mx) - base;
             ws_reg[jj] = ws;
           }
         }
@@ -693,7 +692,6 @@ k_dmt_wl(const WlArgs w) {
       const int nc = min(SLAB, it.nchans - k * SLAB);
       const float* sd = reinterpret_cast<const float*>(sdata) + (int64_t)s * SLAB * w.slot_w;
       const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
-      const int32_t* bs = sbase + s * SLAB;
       // SPP_ACC_KAHAN32: a plain fp32 partial over the slab (<= 32 channels),
       // then one compensated (Kahan) step per slab into the running sum
       float p_acc[R];
@@ -701,7 +699,7 @@ k_dmt_wl(const WlArgs w) {
       for (int r = 0; r < R; ++r) p_acc[r] = 0.f;
 #pragma unroll 4
       for (int j = 0; j < nc; ++j) {
-        const float* row = sd + j * w.slot_w + (wbase + dl[j] - bs[j]);
+        const float* row = sd + j * w.slot_w + (wbase + dl[j]);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const float x = row[32 * r];
@@ -749,12 +747,11 @@ k_dmt_wl(const WlArgs w) {
       const int nc = min(SLAB, it.nchans - k * SLAB);
       const uint32_t* sd = sdata + (int64_t)s * SLAB * w.slot_w;
       const int32_t* dl = sdel + (s * DW + dmw) * SLAB;
-      const int32_t* bs = sbase + s * SLAB;
       for (int jb = 0; jb < nc; jb += F8) {
         const int je = min(nc, jb + F8);
 #pragma unroll 4
         for (int j = jb; j < je; ++j) {
-          const int o = dl[j] - bs[j];
+          const int o = dl[j];
           const uint32_t* row = sd + j * w.slot_w + (o >> P::kLogSpw) + wbase;
           const int sh = (o & (SPW - 1)) * NB;
 #pragma unroll
