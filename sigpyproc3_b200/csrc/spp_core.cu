@@ -129,6 +129,9 @@ static const std::vector<Variant>& variants() {
       mk<32, 8, 4, 1, 16, 2, SPP_ACC_KAHAN32>(0),
       mk<32, 4, 1, 4, 32, 2, SPP_ACC_KAHAN32>(1),
       mk<32, 2, 1, 4, 32, 2, SPP_ACC_KAHAN32>(1),
+      mk<32, 16, 4, 1, 16, 2, SPP_ACC_KAHAN32>(0),
+      mk<32, 8, 2, 1, 16, 2, SPP_ACC_KAHAN32>(0),
+      mk<32, 16, 2, 1, 16, 2, SPP_ACC_KAHAN32>(0),
       // float32 input, fp64 accumulator
       mk<32, 8, 8, 1, 32, 2, SPP_ACC_F64>(0),
       mk<32, 4, 8, 2, 32, 2, SPP_ACC_F64>(0),
