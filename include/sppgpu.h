@@ -176,7 +176,7 @@ int spp_dmt_execute_zero_dm(const spp_dmt_plan* plan, const float* in, int64_t n
 /* Same transform end to end from HOST memory: `in_host` (pinned or pageable)
  * and `out_host` (ndm x out_stride elements).  Time is cut into blocks of
  * `block_nsamps` output samples; H2D, compute and D2H of successive blocks
- * overlap on two internal streams.  Synchronous: returns when out_host is
+ * overlap on three internal streams.  Synchronous: returns when out_host is
  * complete. */
 int spp_dmt_execute_host(const spp_dmt_plan* plan, const void* in_host,
                          int64_t nsamps, void* out_host, int64_t out_stride,

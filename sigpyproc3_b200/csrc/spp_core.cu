@@ -842,9 +842,13 @@ static HostLayout host_layout(const spp_dmt_plan* p, int64_t block) {
   return h;
 }
 
+// Host streaming keeps this many block buffer sets (and streams) in flight:
+// copies in, DM kernel and copies out of consecutive blocks overlap.
+constexpr int kHostSets = 3;
+
 int64_t spp_dmt_host_workspace_bytes(const spp_dmt_plan* p, int64_t block_nsamps) {
   if (!p || block_nsamps <= 0) return -1;
-  return kStatusBytes + 2 * host_layout(p, block_nsamps).set_bytes;
+  return kStatusBytes + kHostSets * host_layout(p, block_nsamps).set_bytes;
 }
 
 int spp_dmt_execute_host(const spp_dmt_plan* p, const void* in_host, int64_t nsamps,
@@ -860,20 +864,24 @@ int spp_dmt_execute_host(const spp_dmt_plan* p, const void* in_host, int64_t nsa
   const HostLayout h = host_layout(p, block_nsamps);
   if (h.in_rows > p->nsamps_max)
     return fail(SPP_ERR_SIZE, "block + max delay (%lld) exceeds plan nsamps_max", (long long)h.in_rows);
-  if (workspace_bytes < kStatusBytes + 2 * h.set_bytes) return fail(SPP_ERR_SIZE, "workspace too small");
+  if (workspace_bytes < kStatusBytes + kHostSets * h.set_bytes)
+    return fail(SPP_ERR_SIZE, "workspace too small");
   if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return fail(SPP_ERR_ALIGN, "workspace must be 256-B aligned");
   uint8_t* ws = static_cast<uint8_t*>(workspace);
-  cudaStream_t s[2];
+  cudaStream_t s[kHostSets];
   int rc = SPP_OK;
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < kHostSets; ++i) {
     rc = cuda_status(cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking), "stream create");
-    if (rc) { if (i) cudaStreamDestroy(s[0]); return rc; }
+    if (rc) {
+      for (int j = 0; j < i; ++j) cudaStreamDestroy(s[j]);
+      return rc;
+    }
   }
   const int64_t rb = host_row_bytes(p);
   const int64_t es = 4;
   const int64_t nblocks = ceil_div(nvalid, block_nsamps);
   for (int64_t b = 0; b < nblocks && rc == SPP_OK; ++b) {
-    const int k = (int)(b & 1);
+    const int k = (int)(b % kHostSets);
     uint8_t* set = ws + kStatusBytes + k * h.set_bytes;
     uint8_t* d_in = set;
     uint8_t* d_out = set + h.in_bytes;
@@ -890,7 +898,7 @@ int spp_dmt_execute_host(const spp_dmt_plan* p, const void* in_host, int64_t nsa
                                        d_out, nout * es, nout * es, p->ndm,
                                        cudaMemcpyDeviceToHost, s[k]), "D2H");
   }
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < kHostSets; ++i) {
     int r2 = cuda_status(cudaStreamSynchronize(s[i]), "stream sync");
     if (!rc) rc = r2;
     cudaStreamDestroy(s[i]);
