@@ -220,9 +220,11 @@ class DMTPlan:
         self.set_variant(best)
         rec = {"variant": best, "ms": times[best], "all_ms": times, "shape": self.describe()}
         table[key] = rec
-        try:
+        try:  # atomic replace: processes tuning at once never leave a torn file
             path.parent.mkdir(parents=True, exist_ok=True)
-            path.write_text(json.dumps(table, indent=1))
+            tmp = path.with_name(f"{path.name}.{os.getpid()}.tmp")
+            tmp.write_text(json.dumps(table, indent=1))
+            os.replace(tmp, path)
         except OSError:
             pass
         return rec
