@@ -112,7 +112,7 @@ def load() -> ctypes.CDLL:
         return _LIB
     if not LIB_PATH.exists():
         raise ImportError(
-            f"{LIB_PATH} is missing: build it with `python -m sigpyproc3_b200._build` "
+            f"{LIB_PATH} is missing: build it with `python sigpyproc3_b200/_build.py` "
             "(there is no CPU fallback)"
         )
     try:
