@@ -147,8 +147,8 @@ __global__ void k_subband(const void* __restrict__ in, int64_t nchans, int64_t n
 // chunk's sum and second central moment.  Final pass merges chunks (Chan et
 // al. 1979 pairwise variance) and forms (best - w*mean) / (std*sqrt(w)).
 // ---------------------------------------------------------------------------
-constexpr int kSnrChunk = 4096;
-constexpr int kSnrThreads = 512;
+constexpr int kSnrChunk = 8192;     // downsampled samples per CTA (32 per thread)
+constexpr int kSnrThreads = 256;
 constexpr int kSnrMaxW = 4096;
 constexpr int kSnrMaxWidths = 32;
 
@@ -168,13 +168,20 @@ __device__ __forceinline__ double row_val(const void* in, int kind, int64_t i) {
                              : (double)static_cast<const float*>(in)[i];
 }
 
+// One CTA per (chunk of kSnrChunk downsampled samples, row, factor).  Chunk-
+// local indices are 32-bit; the width maxima keep per-thread candidates for up
+// to kSnrWGroup widths in registers over one pass of the chunk, then reduce
+// once (ties go to the smaller sample index, as the reference's argmax).
+constexpr int kSnrWGroup = 12;
+
 __global__ void __launch_bounds__(kSnrThreads)
 k_snr_chunk(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride, const SnrCfg cfg,
             int64_t nchunks, SnrPart* __restrict__ parts, double* __restrict__ stats) {
   const int nfactors = cfg.nf, nwidths = cfg.nw, wmax = cfg.wmax;
   extern __shared__ double sy[];  // kSnrChunk + wmax + 1
-  __shared__ double red_d[kSnrThreads / 32];
-  __shared__ long long red_i[kSnrThreads / 32];
+  __shared__ double red_d[kSnrThreads / 32 * kSnrWGroup];
+  __shared__ int red_i[kSnrThreads / 32 * kSnrWGroup];
+  __shared__ int sw[kSnrMaxWidths];
   __shared__ double carry;
   const int64_t k = blockIdx.x;
   const int64_t row = blockIdx.y / nfactors;
@@ -185,25 +192,30 @@ k_snr_chunk(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
   if (i0 >= m) {
     return;
   }
-  const int64_t own = imin64(kSnrChunk, m - i0);
-  const int64_t len = imin64(own + wmax, m - i0);  // samples loaded
+  const int own = (int)imin64(kSnrChunk, m - i0);
+  const int len = (int)imin64(own + wmax, m - i0);  // samples loaded
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x < nwidths) sw[threadIdx.x] = cfg.w[threadIdx.x];
   const char* base = static_cast<const char*>(in) + row * in_stride * 4;
-  // y values (downsampled means rounded to float32 as the reference output dtype)
-  for (int64_t j = threadIdx.x; j < len; j += blockDim.x) {
+  // y values (downsampled means rounded to float32 as the reference output
+  // dtype); a power-of-two factor divides exactly by multiplying
+  const bool pow2 = (f & (f - 1)) == 0;
+  const double inv = 1.0 / (double)f;
+  for (int j = threadIdx.x; j < len; j += blockDim.x) {
     double s = 0.0;
     const int64_t x0 = (i0 + j) * f;
     for (int q = 0; q < f; ++q) s += row_val(base, kind, x0 + q);
-    sy[j + 1] = (double)(float)(s / f);
+    sy[j + 1] = (double)(float)(pow2 ? s * inv : s / f);
   }
   if (threadIdx.x == 0) { sy[0] = 0.0; carry = 0.0; }
   __syncthreads();
   // chunk sum and M2 over owned samples
   {
     double s = 0.0;
-    for (int64_t j = threadIdx.x; j < own; j += blockDim.x) s += sy[j + 1];
+    for (int j = threadIdx.x; j < own; j += blockDim.x) s += sy[j + 1];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red_d[threadIdx.x >> 5] = s;
+    if (lane == 0) red_d[warp] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
@@ -213,14 +225,14 @@ k_snr_chunk(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
     __syncthreads();
     const double mu = carry / (double)own;
     double q = 0.0;
-    for (int64_t j = threadIdx.x; j < own; j += blockDim.x) {
+    for (int j = threadIdx.x; j < own; j += blockDim.x) {
       const double d = sy[j + 1] - mu;
       q += d * d;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
     __syncthreads();
-    if ((threadIdx.x & 31) == 0) red_d[threadIdx.x >> 5] = q;
+    if (lane == 0) red_d[warp] = q;
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
@@ -234,14 +246,12 @@ k_snr_chunk(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
   }
   // inclusive scan of sy[1..len] (sequential per thread segment + warp/block scan)
   {
-    const int64_t per = (len + blockDim.x - 1) / blockDim.x;
-    const int64_t a = 1 + threadIdx.x * per;
-    const int64_t b = imin64(a + per, len + 1);
+    const int per = (len + blockDim.x - 1) / blockDim.x;
+    const int a = 1 + threadIdx.x * per;
+    const int b = min(a + per, len + 1);
     double s = 0.0;
-    for (int64_t j = a; j < b; ++j) { s += sy[j]; sy[j] = s; }
-    // exclusive scan of segment totals across threads
+    for (int j = a; j < b; ++j) { s += sy[j]; sy[j] = s; }
     double incl = s;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const double v = __shfl_up_sync(0xffffffffu, incl, o);
@@ -255,35 +265,52 @@ k_snr_chunk(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
     }
     __syncthreads();
     const double off = red_d[warp] + (incl - s);
-    for (int64_t j = a; j < b; ++j) sy[j] += off;
+    for (int j = a; j < b; ++j) sy[j] += off;
     __syncthreads();
   }
-  // window maxima per width
-  for (int wi = 0; wi < nwidths; ++wi) {
-    const int w = cfg.w[wi];
-    double best = -DBL_MAX;
-    long long bidx = LLONG_MAX;
-    for (int64_t t = threadIdx.x; t < own; t += blockDim.x) {
-      if (t + w > len) break;  // beyond the row end (len == m - i0 there)
-      const double v = sy[t + w] - sy[t];
-      if (v > best) { best = v; bidx = i0 + t; }
+  // window maxima: widths in groups of kSnrWGroup, one pass over the chunk each
+  for (int w0 = 0; w0 < nwidths; w0 += kSnrWGroup) {
+    double best[kSnrWGroup];
+    int bt[kSnrWGroup], wv[kSnrWGroup];
+#pragma unroll
+    for (int g = 0; g < kSnrWGroup; ++g) {
+      best[g] = -DBL_MAX;
+      bt[g] = INT_MAX;
+      wv[g] = (w0 + g < nwidths) ? sw[w0 + g] : INT_MAX / 2;
+    }
+    for (int t = threadIdx.x; t < own; t += blockDim.x) {
+      const double p0 = sy[t];
+#pragma unroll
+      for (int g = 0; g < kSnrWGroup; ++g) {
+        if (t + wv[g] <= len) {  // window inside the loaded samples
+          const double v = sy[t + wv[g]] - p0;
+          if (v > best[g]) { best[g] = v; bt[g] = t; }
+        }
+      }
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-      const long long oi = __shfl_xor_sync(0xffffffffu, bidx, o);
-      if (ov > best || (ov == best && oi < bidx)) { best = ov; bidx = oi; }
+    for (int g = 0; g < kSnrWGroup; ++g) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best[g], o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bt[g], o);
+        if (ov > best[g] || (ov == best[g] && oi < bt[g])) { best[g] = ov; bt[g] = oi; }
+      }
+      if (lane == 0) { red_d[warp * kSnrWGroup + g] = best[g]; red_i[warp * kSnrWGroup + g] = bt[g]; }
     }
-    if ((threadIdx.x & 31) == 0) { red_d[threadIdx.x >> 5] = best; red_i[threadIdx.x >> 5] = bidx; }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      best = red_d[0];
-      bidx = red_i[0];
-      for (int w2 = 1; w2 < kSnrThreads / 32; ++w2)
-        if (red_d[w2] > best || (red_d[w2] == best && red_i[w2] < bidx)) { best = red_d[w2]; bidx = red_i[w2]; }
-      SnrPart* p = parts + (((row * nfactors + fi) * nwidths + wi) * nchunks + k);
-      p->best = best;
-      p->idx = bidx;
+    if (threadIdx.x < kSnrWGroup && w0 + (int)threadIdx.x < nwidths) {
+      const int g = threadIdx.x;
+      double bb = red_d[g];
+      int bi = red_i[g];
+      for (int w2 = 1; w2 < kSnrThreads / 32; ++w2) {
+        const double v = red_d[w2 * kSnrWGroup + g];
+        const int vi = red_i[w2 * kSnrWGroup + g];
+        if (v > bb || (v == bb && vi < bi)) { bb = v; bi = vi; }
+      }
+      SnrPart* p = parts + (((row * nfactors + fi) * nwidths + (w0 + g)) * nchunks + k);
+      p->best = bb;
+      p->idx = bi == INT_MAX ? LLONG_MAX : i0 + bi;
     }
     __syncthreads();
   }

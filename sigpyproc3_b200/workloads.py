@@ -19,7 +19,8 @@ def _events():
 
 
 def run(name: str, args, rank: int, world: int, local: int, emit) -> None:
-    {"c1": run_c1, "c4": run_c4, "c5": run_c5}[name](args, rank, world, local, emit)
+    {"c1": run_c1, "c4": run_c4, "c5": run_c5, "snr": run_snr}[name](args, rank, world, local,
+                                                                      emit)
 
 
 def run_c1(args, rank, world, local, emit) -> None:
@@ -270,3 +271,42 @@ def run_c5(args, rank, world, local, emit) -> None:
              kernel_ms={"dmt": dmt_ms, "corner_turn_zero_dm": tk["ms_corner_turn"] / max(tk["n"], 1)},
              fp32_adds_per_s=adds / (dmt_ms / 1e3), max_snr=float(snr.max()))
     plan.close()
+
+
+def run_snr(args, rank, world, local, emit) -> None:
+    """The boxcar S/N epilogue alone (R8 + R9) on a config-3-shaped DM-time
+    block: 512 int32 rows x 2^20 samples, downsample 1/2/4, widths 1..256."""
+    import json
+    from pathlib import Path
+
+    from .search import boxcar_snr
+
+    nrows, n = args.ndm or 512, args.nsamps or (1 << 20)
+    rows = synth.uniform_bytes_device(nrows * n * 4, 9).view(torch.int32).view(nrows, n)
+    rows.bitwise_and_(0x3FFF)  # values of a 1024-channel 8-bit sum range
+    factors, widths = (1, 2, 4), tuple(1 << k for k in range(9))
+    snr = torch.empty((nrows, 3, 9), dtype=torch.float32, device="cuda")
+    idx = torch.empty_like(snr, dtype=torch.int32)
+    for _ in range(max(args.warmup, 1)):
+        boxcar_snr(rows, widths=widths, factors=factors, out=(snr, idx))
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    for _ in range(max(args.steps, 1)):
+        boxcar_snr(rows, widths=widths, factors=factors, out=(snr, idx))
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    alg = nrows * n * 4 * len(factors) + snr.numel() * 8  # each factor reads the rows once
+    pk = Path(__file__).resolve().parents[1] / "MEASURED_PEAKS.json"
+    peak = json.loads(pk.read_text())["hbm_gbs"] if pk.exists() else 6650.0
+    if rank == 0:
+        emit(metric="row-samples/s, boxcar S/N epilogue (downsample 1/2/4 x widths 1..256)",
+             value=nrows * n / (ms / 1e3), unit="row-samples/s", n_gpus=world,
+             steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True,
+             scaling="weak", vs_baseline=None, dtype="int32 -> f64 sums -> f32 S/N",
+             data="synthetic uniform int32 rows on device (seed 9)",
+             config={"workload": f"S/N epilogue: {nrows} rows x {n} samples (config-3 rows)"},
+             roofline={"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak,
+                       "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak,
+                       "algorithmic_bytes": alg})
