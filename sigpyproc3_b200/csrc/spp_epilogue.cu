@@ -278,18 +278,34 @@ k_snr_chunk(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
       bt[g] = INT_MAX;
       wv[g] = (w0 + g < nwidths) ? sw[w0 + g] : INT_MAX / 2;
     }
-    for (int t = threadIdx.x; t < own; t += blockDim.x) {
-      const double p0 = sy[t];
+    const int ng = min(kSnrWGroup, nwidths - w0);
+    if (len == own + wmax) {
+      // interior chunk: every window of every owned sample is loaded
+      for (int t = threadIdx.x; t < own; t += blockDim.x) {
+        const double p0 = sy[t];
 #pragma unroll
-      for (int g = 0; g < kSnrWGroup; ++g) {
-        if (t + wv[g] <= len) {  // window inside the loaded samples
-          const double v = sy[t + wv[g]] - p0;
-          if (v > best[g]) { best[g] = v; bt[g] = t; }
+        for (int g = 0; g < kSnrWGroup; ++g) {
+          if (g < ng) {
+            const double v = sy[t + wv[g]] - p0;
+            if (v > best[g]) { best[g] = v; bt[g] = t; }
+          }
+        }
+      }
+    } else {
+      for (int t = threadIdx.x; t < own; t += blockDim.x) {
+        const double p0 = sy[t];
+#pragma unroll
+        for (int g = 0; g < kSnrWGroup; ++g) {
+          if (t + wv[g] <= len) {  // window inside the row
+            const double v = sy[t + wv[g]] - p0;
+            if (v > best[g]) { best[g] = v; bt[g] = t; }
+          }
         }
       }
     }
 #pragma unroll
     for (int g = 0; g < kSnrWGroup; ++g) {
+      if (g >= ng) break;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         const double ov = __shfl_xor_sync(0xffffffffu, best[g], o);
