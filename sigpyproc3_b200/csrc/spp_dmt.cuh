@@ -888,36 +888,40 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
     uint32_t cq[4][P];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {    // 4 channels
-      uint32_t x[NB][4][P];
+      // per channel: staged row start and bit shift, decoded once
+      const uint32_t* base[4];
+      int sh[4];
+      bool live[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int j = 16 * m + 4 * i + q;
-        const bool live = FULL || j < nc;
-        const int2 ow = live ? off[j] : make_int2(0, 0);  // (word, bit shift)
-        const int sh = ow.y;
-        const uint32_t* base = sd + j * NB * slot_w + ow.x + wbase;
-#pragma unroll
-        for (int b = 0; b < NB; ++b) {
-#pragma unroll
-          for (int p = 0; p < P; ++p) {
-            uint32_t lo = 0u, hi = 0u;
-            if (live) {
-              lo = base[b * slot_w + 32 * p];
-              hi = base[b * slot_w + 32 * p + 1];
-            }
-            x[b][q][p] = __funnelshift_r(lo, hi, sh);
-          }
-        }
+        live[q] = FULL || j < nc;
+        const int2 ow = live[q] ? off[j] : make_int2(0, 0);  // (word, bit shift)
+        sh[q] = ow.y;
+        base[q] = sd + j * NB * slot_w + ow.x + wbase;
       }
+      // one word position at a time: 4 channels x NB planes live, not x P
 #pragma unroll
       for (int p = 0; p < P; ++p) {
+        uint32_t x[NB][4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+#pragma unroll
+          for (int b = 0; b < NB; ++b) {
+            uint32_t lo = 0u, hi = 0u;
+            if (live[q]) {
+              lo = base[q][b * slot_w + 32 * p];
+              hi = base[q][b * slot_w + 32 * p + 1];
+            }
+            x[b][q] = __funnelshift_r(lo, hi, sh[q]);
+          }
+        }
         if constexpr (NB == 2) {
-          const uint32_t lo[4] = {x[0][0][p], x[0][1][p], x[0][2][p], x[0][3][p]};
-          const uint32_t hi[4] = {x[NB - 1][0][p], x[NB - 1][1][p], x[NB - 1][2][p],
-                                  x[NB - 1][3][p]};
+          const uint32_t lo[4] = {x[0][0], x[0][1], x[0][2], x[0][3]};
+          const uint32_t hi[4] = {x[NB - 1][0], x[NB - 1][1], x[NB - 1][2], x[NB - 1][3]};
           cnt.quad2(p, lo, hi, cq[i][p]);  // weight 16
         } else {
-          const uint32_t v[4] = {x[0][0][p], x[0][1][p], x[0][2][p], x[0][3][p]};
+          const uint32_t v[4] = {x[0][0], x[0][1], x[0][2], x[0][3]};
           cnt.quad1(p, v, cq[i][p]);       // weight 4
         }
       }
