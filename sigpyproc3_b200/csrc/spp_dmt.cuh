@@ -216,7 +216,7 @@ struct IntAcc {
       S[k][1] += v >> 16;
     } else if (NB == 8) {
       E[k][0] += v & 0x00FF00FFu;
-      O[k][0] += (v >> 8) & 0x00FF00FFu;
+      O[k][0] += __byte_perm(v, 0u, 0x4341);  // bytes 1 and 3 into 16-bit lanes
     } else {
 #pragma unroll
       for (int g = 0; g < G; ++g) A[k][g] += (v >> (g * NB)) & P::kMaskByte;
