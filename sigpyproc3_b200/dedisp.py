@@ -92,11 +92,6 @@ def dedisperse_block(raw: torch.Tensor, delays: np.ndarray, nchans: int, nsamps:
     if out.dtype != torch.float32 or not out.is_cuda:
         raise TypeError("out must be a CUDA float32 tensor")
     lib = _lib.load()
-    need = lib.spp_dedisperse_workspace_bytes(nb, nchans, nsamps, dmin, dmax)
-    if need < 0:
-        _lib.check(_lib.SPP_ERR_ARG)
-    if ws is None:
-        ws = workspace(need, raw.device, stream)
     st = stream_handle(stream, raw.device)
     if nb == 8 and host_table is not False:
         rc = lib.spp_dedisperse_hd(raw.data_ptr(), nb, nchans, nsamps, delays.ctypes.data,
@@ -107,6 +102,11 @@ def dedisperse_block(raw: torch.Tensor, delays: np.ndarray, nchans: int, nsamps:
             _lib.check(rc)
     elif host_table:
         raise NotImplementedError("the host-table path covers 8-bit data")
+    need = lib.spp_dedisperse_workspace_bytes(nb, nchans, nsamps, dmin, dmax)
+    if need < 0:
+        _lib.check(_lib.SPP_ERR_ARG)
+    if ws is None:
+        ws = workspace(need, raw.device, stream)
     if delays_dev is None:
         delays_dev = torch.from_numpy(delays).to(raw.device, non_blocking=False)
     _lib.check(lib.spp_dedisperse(
