@@ -285,10 +285,12 @@ def run_c5(args, rank, world, local, emit) -> None:
         emit(metric="DM-trial x samples/s, config 5 (float32 zero-DM + DM-time + boxcar S/N)",
              value=ndm * nv / (ms / 1e3), unit=UNIT, n_gpus=world, steps=args.steps, warmup=1,
              ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
-             dtype="f32 (compensated fp32 sums)", data="synthetic N(0,1) on device (seed 5)",
+             dtype="f32 (fp32 slab partials, compensated sum across slabs)",
+             data="synthetic N(0,1) on device (seed 5)",
              config={"workload": f"config 5: float32 {g.nchans} ch x {nsamps}, zero-DM, {ndm} "
                      "trials 0-3000, boxcar widths 1..512", "tile": plan.describe(),
-                     "accumulator": "fp64" if best[1] == _lib.ACC_F64 else "kahan fp32",
+                     "accumulator": "fp64" if best[1] == _lib.ACC_F64 else
+                     "fp32 slab partials + Kahan across slabs",
                      "autotune_ms": [round(t[0], 2) for t in tune]},
              kernel_ms={"dmt": dmt_ms, "corner_turn_zero_dm": tk["ms_corner_turn"] / max(tk["n"], 1)},
              fp32_adds_per_s=adds / (dmt_ms / 1e3), max_snr=float(snr.max()))
