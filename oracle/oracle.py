@@ -58,6 +58,9 @@ def lib() -> ctypes.CDLL:
             "orc_downsample_mean": ([_p, _i64, ctypes.c_int, _p], None),
             "orc_boxcar_snr_row": ([_p, _i64, _p, ctypes.c_int, _p, ctypes.c_int, _p, _p], None),
             "orc_subband_u8": ([_p, _p, _p, _p, _i64, _i64, _i64, _i64], None),
+            "orc_fold_block": ([_p, ctypes.c_int, _p, _p, _p, _i32, ctypes.c_float,
+                                ctypes.c_float, ctypes.c_float, _i32, _i32, _i32, _i32, _i32,
+                                _i32, _i32], None),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -255,3 +258,41 @@ def read_plan_blocks(nsamples: int, gulp: int = 16384, start: int = 0, nsamps: i
     if lastread != 0:
         blocks.append((nreads, lastread, 0))
     return blocks
+
+
+# ---------------------------------------------------------------------------
+# kernels.fold (core/kernels.py:403-445) and Filterbank.fold (base.py:1109-1207)
+# ---------------------------------------------------------------------------
+def fold_block(data: np.ndarray, fold_ar: np.ndarray, count_ar: np.ndarray, delays: np.ndarray,
+               maxdelay: int, tsamp: float, period: float, accel: float, total_nsamps: int,
+               nsamps: int, nchans: int, nbins: int, nints: int, nsubs: int, index: int) -> None:
+    """One read_plan block of kernels.fold, accumulated into fold_ar / count_ar."""
+    data = np.ascontiguousarray(data)
+    delays = np.ascontiguousarray(delays, dtype=np.int32)
+    if data.dtype not in (np.uint8, np.float32):
+        raise TypeError(data.dtype)
+    lib().orc_fold_block(_ptr(data), int(data.dtype == np.float32), _ptr(fold_ar), _ptr(count_ar),
+                         _ptr(delays), maxdelay, tsamp, period, accel, total_nsamps, nsamps,
+                         nchans, nbins, nints, nsubs, index)
+
+
+def filterbank_fold(data: np.ndarray, nsamples: int, nchans: int, delays: np.ndarray,
+                    tsamp: float, period: float, accel: float, nbins: int, nints: int,
+                    nbands: int, gulp: int):
+    """Filterbank.fold's block loop (base.py:1151-1206) over a time-major array:
+    returns (sums, counts, cube) with the reference's final float32 division."""
+    nbands = min(nbands, nchans)
+    maxd = int(np.max(delays))
+    gulp = max(2 * maxd, gulp)
+    fold_ar = np.zeros(nbins * nints * nbands, dtype=np.float32)
+    count_ar = np.zeros(nbins * nints * nbands, dtype=np.int32)
+    pos = 0
+    for ii, nblk, skip in read_plan_blocks(nsamples, gulp, 0, None, maxd):
+        blk = data[pos * nchans:(pos + nblk) * nchans]
+        fold_block(blk, fold_ar, count_ar, delays, maxd, tsamp, period, accel, nsamples, nblk,
+                   nchans, nbins, nints, nbands, ii * (gulp - maxd))
+        pos += nblk + skip
+    sums, counts = fold_ar.copy(), count_ar.copy()
+    with np.errstate(divide="ignore", invalid="ignore"):
+        fold_ar /= count_ar
+    return sums, counts, fold_ar.reshape(nints, nbands, nbins)

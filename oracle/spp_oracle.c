@@ -284,3 +284,52 @@ void orc_dmt_rowmajor_u8(const uint8_t* in, const int32_t* delays, int64_t ndm, 
     }
   }
 }
+
+/* Python's float floor division a // b (CPython float_floor_div: fmod-based,
+   so the quotient is the floor of the exact quotient), restated. */
+static double py_floordiv(double a, double b) {
+  const double mod = fmod(a, b);
+  double div = (a - mod) / b;
+  if (mod != 0.0 && ((b < 0.0) != (mod < 0.0))) div -= 1.0;
+  if (div == 0.0) return copysign(0.0, a / b);
+  double fl = floor(div);
+  if (div - fl > 0.5) fl += 1.0;
+  return fl;
+}
+
+/* kernels.fold (core/kernels.py:403-445): one read_plan block into fold_ar /
+   count_ar.  The reference takes tsamp, period and accel as float32 and does
+   the phase arithmetic in float64, in this order; the bin sums are float32. */
+static void orc_fold_impl(const void* in, int is_f32, float* fold_ar, int32_t* count_ar,
+                          const int32_t* delays, int32_t maxdelay, float tsamp, float period,
+                          float accel, int32_t total_nsamps, int32_t nsamps, int32_t nchans,
+                          int32_t nbins, int32_t nints, int32_t nsubs, int32_t index) {
+  const double c2 = 2.0 * 299792458.0;
+  const double factor1 = (double)total_nsamps / (double)nints;
+  const double factor2 = (double)nchans / (double)nsubs;
+  const double tobs = (double)total_nsamps * (double)tsamp;
+  for (int64_t isamp = 0; isamp < (int64_t)nsamps - maxdelay; ++isamp) {
+    const double tj = (double)(isamp + index) * (double)tsamp;
+    const double phase =
+        (double)nbins * tj * (1.0 + (double)accel * (tj - tobs) / c2) / (double)period + 0.5;
+    const int64_t phasebin = llabs((long long)phase) % nbins;
+    const double subint = py_floordiv((double)(isamp + index), factor1);
+    const double pos1 = subint * nbins * nsubs + (double)phasebin;
+    for (int64_t ichan = 0; ichan < nchans; ++ichan) {
+      const double sub_band = py_floordiv((double)ichan, factor2);
+      const int64_t pos2 = (int64_t)(pos1 + sub_band * nbins);
+      const int64_t idx = (int64_t)nchans * (isamp + delays[ichan]) + ichan;
+      const float val = is_f32 ? ((const float*)in)[idx] : (float)((const uint8_t*)in)[idx];
+      fold_ar[pos2] = fold_ar[pos2] + val;
+      count_ar[pos2] += 1;
+    }
+  }
+}
+
+void orc_fold_block(const void* in, int is_f32, float* fold_ar, int32_t* count_ar,
+                    const int32_t* delays, int32_t maxdelay, float tsamp, float period,
+                    float accel, int32_t total_nsamps, int32_t nsamps, int32_t nchans,
+                    int32_t nbins, int32_t nints, int32_t nsubs, int32_t index) {
+  orc_fold_impl(in, is_f32, fold_ar, count_ar, delays, maxdelay, tsamp, period, accel,
+                total_nsamps, nsamps, nchans, nbins, nints, nsubs, index);
+}

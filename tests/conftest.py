@@ -31,3 +31,22 @@ def orc():
 
     oracle.build()
     return oracle
+
+
+@pytest.fixture(scope="session")
+def fold_input():
+    """Regenerates the seeded input of a golden fold case (tests/golden/make_golden.py)
+    and checks it against the recorded sha256."""
+    import hashlib
+
+    def make(case):
+        rng = np.random.default_rng(case["seed"])
+        n = case["nsamples"] * case["nchans"]
+        if case["dtype"] == "uint8":
+            data = rng.integers(0, 256, size=n, dtype=np.uint8)
+        else:
+            data = rng.normal(0.0, 1.0, size=n).astype(np.float32)
+        assert hashlib.sha256(data.tobytes()).hexdigest() == case["input_sha256"]
+        return data
+
+    return make

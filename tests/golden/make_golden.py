@@ -258,6 +258,45 @@ def main() -> None:
     for f in (1, 2, 4, 7):
         out[f"ds_out_{f}"] = K.downsample_1d_mean(ds_in, f)
 
+    # ---- N4 kernels.fold through the Filterbank.fold block loop (base.py:1151-1206)
+    fold_cases = []
+    for tag, dtype, nsamples, period, dm, accel, nbins, nints, nbands, gulp, seed in (
+        ("a", np.uint8, 12000, 0.0313, 40.0, 0.0, 50, 8, 8, 2048, 21),
+        ("b", np.uint8, 9000, 0.0251, 15.0, 30.0, 37, 7, 5, 1500, 22),
+        ("c", np.float32, 6000, 0.0199, 25.0, -12.0, 23, 5, 6, 1024, 23),
+    ):
+        nch, tsamp = 64, 320e-6
+        rng = np.random.default_rng(seed)
+        if dtype == np.uint8:
+            data_all = rng.integers(0, 256, size=nsamples * nch, dtype=np.uint8)
+        else:
+            data_all = rng.normal(0.0, 1.0, size=nsamples * nch).astype(np.float32)
+        itemsize = np.dtype(dtype).itemsize
+        fr = FakeReader(data_all.view(np.uint8), nsamples, nch, itemsize)
+        fr.bitsinfo.dtype = np.dtype(dtype)
+        nb = min(nbands, nch)
+        cd = ref_delays(nch, 1510.0, -1.09, tsamp, dm).astype(np.int32)
+        maxd = int(cd.max())
+        g = max(2 * maxd, gulp)
+        fold_ar = np.zeros(nbins * nints * nb, dtype=np.float32)
+        count_ar = np.zeros(nbins * nints * nb, dtype=np.int32)
+        for nsamps_r, ii, data in read_plan(fr, gulp=g, skipback=maxd, quiet=True):
+            K.fold(np.ascontiguousarray(data), fold_ar, count_ar, cd, np.int32(maxd),
+                   np.float32(tsamp), np.float32(period), np.float32(accel), np.int32(nsamples),
+                   np.int32(nsamps_r), np.int32(nch), np.int32(nbins), np.int32(nints),
+                   np.int32(nb), np.int32(ii * (g - maxd)))
+        out[f"fold_{tag}_sum"] = fold_ar.copy()
+        out[f"fold_{tag}_count"] = count_ar.copy()
+        with np.errstate(divide="ignore", invalid="ignore"):
+            fold_ar /= count_ar
+        out[f"fold_{tag}_cube"] = fold_ar.reshape(nints, nb, nbins)
+        fold_cases.append({"tag": tag, "dtype": np.dtype(dtype).name, "nsamples": nsamples,
+                           "nchans": nch, "tsamp": tsamp, "fch1": 1510.0, "foff": -1.09,
+                           "period": period, "dm": dm, "accel": accel, "nbins": nbins,
+                           "nints": nints, "nbands": nbands, "gulp": gulp, "seed": seed,
+                           "input_sha256": sha(data_all)})
+    meta["fold_cases"] = fold_cases
+
     np.savez_compressed(HERE / "golden.npz", **out)
     (HERE / "golden.json").write_text(json.dumps(meta, indent=1))
     print(f"wrote {len(out)} arrays, {(HERE / 'golden.npz').stat().st_size} bytes")

@@ -111,3 +111,19 @@ def test_boxcar_snr_small(orc):
             s = np.array([y[t:t + w].sum() for t in range(y.size - w + 1)])
             assert idx[0, fi, wi] == int(np.argmax(s))
             assert np.isclose(snr[0, fi, wi], (s.max() - w * mu) / (sd * np.sqrt(w)), rtol=1e-12)
+
+
+@pytest.mark.parametrize("tag", ["a", "b", "c"])
+def test_fold(orc, golden, golden_meta, fold_input, tag):
+    """kernels.fold through Filterbank.fold's block loop, against the reference's
+    own output: sums, counts and the divided cube, bit for bit."""
+    case = next(c for c in golden_meta["fold_cases"] if c["tag"] == tag)
+    data = fold_input(case)
+    freqs = orc.chan_freqs(case["nchans"], case["fch1"], case["foff"])
+    d = np.atleast_1d(orc.dmdelays(freqs, case["dm"], case["tsamp"], case["fch1"])).astype(np.int32)
+    sums, counts, cube = orc.filterbank_fold(
+        data, case["nsamples"], case["nchans"], d, case["tsamp"], case["period"], case["accel"],
+        case["nbins"], case["nints"], case["nbands"], case["gulp"])
+    np.testing.assert_array_equal(counts, golden[f"fold_{tag}_count"])
+    np.testing.assert_array_equal(sums, golden[f"fold_{tag}_sum"])
+    np.testing.assert_array_equal(cube, golden[f"fold_{tag}_cube"])
