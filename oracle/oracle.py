@@ -58,6 +58,7 @@ def lib() -> ctypes.CDLL:
             "orc_downsample_mean": ([_p, _i64, ctypes.c_int, _p], None),
             "orc_boxcar_snr_row": ([_p, _i64, _p, ctypes.c_int, _p, ctypes.c_int, _p, _p], None),
             "orc_subband_u8": ([_p, _p, _p, _p, _i64, _i64, _i64, _i64], None),
+            "orc_py_floordiv": ([ctypes.c_double, ctypes.c_double], ctypes.c_double),
             "orc_fold_block": ([_p, ctypes.c_int, _p, _p, _p, _i32, ctypes.c_float,
                                 ctypes.c_float, ctypes.c_float, _i32, _i32, _i32, _i32, _i32,
                                 _i32, _i32], None),

@@ -318,7 +318,8 @@ static void orc_fold_impl(const void* in, int is_f32, float* fold_ar, int32_t* c
     for (int64_t ichan = 0; ichan < nchans; ++ichan) {
       const double sub_band = py_floordiv((double)ichan, factor2);
       const int64_t pos2 = (int64_t)(pos1 + sub_band * nbins);
-      const int64_t idx = (int64_t)nchans * (isamp + delays[ichan]) + ichan;
+      int64_t idx = (int64_t)nchans * (isamp + delays[ichan]) + ichan;
+      if (idx < 0) idx += (int64_t)nsamps * nchans;  /* numba: negative index wraps */
       const float val = is_f32 ? ((const float*)in)[idx] : (float)((const uint8_t*)in)[idx];
       fold_ar[pos2] = fold_ar[pos2] + val;
       count_ar[pos2] += 1;
@@ -333,3 +334,6 @@ void orc_fold_block(const void* in, int is_f32, float* fold_ar, int32_t* count_a
   orc_fold_impl(in, is_f32, fold_ar, count_ar, delays, maxdelay, tsamp, period, accel,
                 total_nsamps, nsamps, nchans, nbins, nints, nsubs, index);
 }
+
+/* The floor division above, exported for its test against Python's own //. */
+double orc_py_floordiv(double a, double b) { return py_floordiv(a, b); }

@@ -127,3 +127,23 @@ def test_fold(orc, golden, golden_meta, fold_input, tag):
     np.testing.assert_array_equal(counts, golden[f"fold_{tag}_count"])
     np.testing.assert_array_equal(sums, golden[f"fold_{tag}_sum"])
     np.testing.assert_array_equal(cube, golden[f"fold_{tag}_cube"])
+
+
+def test_py_floordiv_matches_python(orc):
+    """The restated float floor division (fold's subintegration and subband
+    indices) equals Python's own // -- random operands and quotients that land
+    on or next to integers."""
+    import math
+
+    rng = np.random.default_rng(41)
+    a = np.concatenate([rng.integers(0, 2**31, 2000).astype(np.float64),
+                        rng.normal(0, 1e6, 2000), np.arange(0, 5000, dtype=np.float64)])
+    b = np.concatenate([rng.uniform(0.1, 5000.0, 2000), rng.normal(0, 100.0, 2000),
+                        np.full(5000, 65536 / 31), ])
+    b[b == 0] = 1.0
+    extra = [(7.0, 0.1), (1.0, 0.1), (0.3, 0.1), (-7.0, 0.1), (6.0, 0.2), (65535.0, 65536 / 32),
+             (12000.0, 12000 / 7), (9000.0 - 1, 9000 / 7), (5.0, -2.0), (-5.0, 2.0), (0.0, 3.0)]
+    for x, y in list(zip(a, b)) + extra:
+        got = orc.lib().orc_py_floordiv(float(x), float(y))
+        want = float(x) // float(y)
+        assert got == want and math.copysign(1, got) == math.copysign(1, want), (x, y, got, want)
