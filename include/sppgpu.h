@@ -110,6 +110,26 @@ int spp_dedisperse_hd(const void* in, int nbits, int64_t nchans, int64_t nsamps,
                       const int32_t* delays_host, float* out, int64_t out_len,
                       int64_t out_start, void* stream);
 
+/* ---- folding -------------------------------------------------------------
+ * Replaces kernels.fold (core/kernels.py:403-445) for one read_plan block
+ * (Filterbank.fold, base.py:1109-1207): sample t of the block (t < nsamps -
+ * maxdelay, global time index + t) of channel c, read at row t + delays[c],
+ * is added into fold_ar[(subint * nsubs + band) * nbins + phasebin] and
+ * counted in count_ar, with the reference's float64 phase arithmetic on the
+ * float32 tsamp / period / accel it receives and Python's float floor
+ * division for the subintegration.  `band_start` (device, nsubs + 1 int32)
+ * gives each subband's first channel as the reference's `ichan // (nchans /
+ * nsubs)` assigns them.  `in`: time-major uint8 (nbits 8) or float32 (nbits
+ * 32) on the device; fold_ar / count_ar (device, `cells` >= nints * nsubs *
+ * nbins entries) accumulate across calls.  uint8 sums are exact while a cell
+ * stays below 2^24, hence equal to the reference's float32 cells; float32
+ * sums differ from its sequential adds by rounding only. */
+int spp_fold(const void* in, int nbits, int64_t nchans, int64_t nsamps,
+             const int32_t* delays, int32_t maxdelay, float tsamp, float period,
+             float accel, int64_t total_nsamps, int32_t nbins, int32_t nints,
+             int32_t nsubs, int64_t index, const int32_t* band_start, float* fold_ar,
+             int32_t* count_ar, int64_t cells, void* stream);
+
 /* Same computation as spp_dedisperse, but allocating nothing and taking no
  * workspace.  No counterpart in the reference.  It serves callers that must not
  * allocate device memory while running (a real-time pipeline that reserves its

@@ -20,6 +20,7 @@ import torch
 from . import _lib
 from .block import FilterbankBlock
 from .dedisp import DMTPlan, dedisperse_block, stream_handle, workspace
+from .folded import FoldedData
 from .header import Header
 from .io.bits import bitorder_code
 from .io.bits import unpack as gpu_unpack
@@ -250,6 +251,62 @@ class Filterbank:
         if method == "mean":
             tim /= h.nchans
         return TimeSeries(tim, h.new_header({"nchans": 1, "dm": 0}))
+
+    # --- N4: folding ---
+    def fold(self, period: float, dm: float, accel: float = 0, nbins: int = 50, nints: int = 32,
+             nbands: int = 32, gulp: int = 16384, start: int = 0, nsamps: int | None = None,
+             **plan_kwargs) -> FoldedData:
+        """Fold into (subintegration, subband, phase bin) cells (base.py:1109-1207).
+
+        The same checks, warnings, block plan and block index as the reference;
+        each block folds on the GPU (``spp_fold``; packed data is unpacked on the
+        device first) into device cells, divided by the counts at the end.
+        """
+        import warnings
+
+        h = self.header
+        if np.isclose(np.modf(period / h.tsamp)[0], 0.001, atol=0):
+            warnings.warn("Foldng interval is an integer multiple of the sampling time",
+                          stacklevel=2)
+        if nbins > period / h.tsamp:
+            warnings.warn("Number of phase bins is greater than period/sampling time",
+                          stacklevel=2)
+        if (h.nsamples * h.nchans) // (nbands * nints * nbins) < 10:
+            raise ValueError(f"nbands x nints x nbins is too large: {nbands * nints * nbins}")
+        nbands = min(nbands, h.nchans)
+        chan_delays = np.atleast_1d(h.get_dmdelays(dm)).astype(np.int32)
+        max_delay = int(chan_delays.max())
+        gulp = max(2 * max_delay, gulp)
+        # subband of each channel as the reference assigns it: ichan // (nchans / nsubs)
+        factor2 = h.nchans / nbands
+        band = np.array([int(c // factor2) for c in range(h.nchans)], dtype=np.int64)
+        if np.any(np.diff(band) < 0) or band.min() < 0 or band.max() >= nbands:
+            raise ValueError("subband assignment out of range")
+        band_start = np.searchsorted(band, np.arange(nbands + 1)).astype(np.int32)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        cells = nbins * nints * nbands
+        fold_ar = torch.zeros(cells, dtype=torch.float32, device=dev)
+        count_ar = torch.zeros(cells, dtype=torch.int32, device=dev)
+        ddev = torch.from_numpy(chan_delays).to(dev)
+        bdev = torch.from_numpy(band_start).to(dev)
+        lib = _lib.load()
+        st = stream_handle(None, dev)
+        for nsamps_r, ii, raw in self.stream_blocks(gulp, start, nsamps, skipback=max_delay,
+                                                    **plan_kwargs):
+            if h.nbits < 8:
+                x, nb = gpu_unpack(raw[:nsamps_r * self.row_bytes], h.nbits, self.bitorder), 8
+            else:
+                x, nb = raw, h.nbits
+            # the reference indexes each block by ii * (gulp - max_delay) (base.py:1202)
+            _lib.check(lib.spp_fold(x.data_ptr(), nb, h.nchans, nsamps_r, ddev.data_ptr(),
+                                    max_delay, h.tsamp, period, accel, h.nsamples, nbins, nints,
+                                    nbands, ii * (gulp - max_delay), bdev.data_ptr(),
+                                    fold_ar.data_ptr(), count_ar.data_ptr(), cells, st))
+        f = fold_ar.cpu().numpy()
+        c = count_ar.cpu().numpy()
+        with np.errstate(divide="ignore", invalid="ignore"):
+            f /= c
+        return FoldedData(f.reshape(nints, nbands, nbins), h.new_header(), period, dm, accel)
 
 
 class FilReader(Filterbank):
