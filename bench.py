@@ -459,7 +459,7 @@ def main():
                     help="output samples per host-streaming block in the e2e leg")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="fix the kernel variant")
-    ap.add_argument("--workload", choices=["c2", "c3", "c4", "c1", "c5", "snr"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c3", "c4", "c1", "c5", "snr", "fold"], default="c2")
     ap.add_argument("--beams", type=int, default=64, help="config 3: number of beams")
     ap.add_argument("--batch", type=int, default=4, help="config 3: beams per graph")
     ap.add_argument("--chunks", type=int, default=128, help="config 4: chunks served")

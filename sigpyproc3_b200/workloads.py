@@ -19,8 +19,8 @@ def _events():
 
 
 def run(name: str, args, rank: int, world: int, local: int, emit) -> None:
-    {"c1": run_c1, "c4": run_c4, "c5": run_c5, "snr": run_snr}[name](args, rank, world, local,
-                                                                      emit)
+    {"c1": run_c1, "c4": run_c4, "c5": run_c5, "snr": run_snr,
+     "fold": run_fold}[name](args, rank, world, local, emit)
 
 
 def run_c1(args, rank, world, local, emit) -> None:
@@ -334,3 +334,36 @@ def run_snr(args, rank, world, local, emit) -> None:
              roofline={"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak,
                        "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak,
                        "algorithmic_bytes": alg})
+
+
+def run_fold(args, rank, world, local, emit) -> None:
+    """Filterbank.fold end to end from host memory: 8-bit 256 channels x 2^20
+    samples (config-1 band, 16x longer), period 50.3 ms, DM 100, the reference's
+    defaults (50 bins, 32 subintegrations, 32 subbands, gulp 16384)."""
+    from .readers import ArrayFilterbank
+
+    g = synth.C1
+    n = 16 * g.nsamps
+    raw = np.random.default_rng(7).integers(0, 256, size=n * g.nchans, dtype=np.uint8)
+    h = Header(nchans=g.nchans, fch1=g.fch1, foff=g.foff, tsamp=g.tsamp, nbits=8, nsamples=n)
+    fb = ArrayFilterbank(raw, h)
+    for _ in range(max(args.warmup, 1)):
+        fb.fold(0.0503, 100.0)
+    torch.cuda.synchronize()
+    reps = max(args.steps, 1)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fd = fb.fold(0.0503, 100.0)
+    dt = (time.perf_counter() - t0) / reps
+    nvalid = n - int(np.atleast_1d(h.get_dmdelays(100.0)).max())
+    if rank == 0:
+        emit(metric="folded samples/s (Filterbank.fold, host array in, cube out)",
+             value=n / dt, unit="samples/s", n_gpus=world, steps=reps, warmup=args.warmup,
+             ms_per_step=dt * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None,
+             dtype="u8 -> f32 cells", data="synthetic uniform bytes (numpy seed 7)",
+             config={"workload": f"fold: 8-bit {g.nchans} ch x {n}, period 50.3 ms, DM 100, "
+                                 "50 bins x 32 subints x 32 subbands, gulp 16384"},
+             e2e={"value": n / dt, "unit": "samples/s", "h2d_bytes_per_step": int(n * g.nchans),
+                  "d2h_bytes_per_step": int(fd.data.nbytes * 2), "ms_per_call": dt * 1e3,
+                  "path": "ArrayFilterbank(host bytes).fold, wall clock"},
+             folded_channel_samples=int(nvalid * g.nchans))
