@@ -45,6 +45,20 @@ class BaseBlock:
     def nsamples(self) -> int:
         return int(self._t.shape[1])
 
+    def pad_samples(self, nsamps_final: int, offset: int, pad_mode: str = "median"):
+        """Pad to ``nsamps_final`` samples per row with each row's median or mean,
+        the block placed at ``offset`` (block.py:108-146).  The pad values come
+        from numpy on the host, as in the reference, so they are the same
+        float32 numbers."""
+        if pad_mode not in {"mean", "median"}:
+            raise ValueError(f"pad_mode must be 'mean' or 'median', got {pad_mode}")
+        data = self.data
+        pad_values = getattr(np, pad_mode)(data, axis=1)
+        data_pad = np.ones((data.shape[0], nsamps_final), dtype=data.dtype)
+        data_pad *= pad_values[:, None]
+        data_pad[:, offset:offset + data.shape[1]] = data
+        return self.__class__(data_pad, self.header.new_header({"nsamples": nsamps_final}))
+
 
 class FilterbankBlock(BaseBlock):
     """(nchans, nsamples) float32 filterbank block held in HBM."""

@@ -384,3 +384,67 @@ class ArrayFilterbank(Filterbank):
         n = max(0, min(view.nbytes, self._raw.nbytes - offset))
         view[:n] = self._raw[offset:offset + n]
         return n
+
+
+class PulseExtractor:
+    """A filterbank block centred on a pulse (readers.py:353-478): the pulse's
+    time of arrival ``pulse_toa`` (samples, at ``toa_freq``, default the top of
+    the band), width and DM fix the window (the DM sweep plus five widths on
+    each side, at least ``min_nsamps`` decimated samples); samples beyond the
+    file are padded with each channel's median or mean."""
+
+    def __init__(self, filfile, pulse_toa: int, pulse_width: int, pulse_dm: float,
+                 min_nsamps: int = 256, toa_freq: float | None = None,
+                 nchans: int | None = None):
+        self.filfile = filfile
+        self.pulse_toa = pulse_toa
+        self.pulse_width = pulse_width
+        self.pulse_dm = pulse_dm
+        self.min_nsamps = min_nsamps
+        hdr = Header.from_sigproc(filfile)
+        self.toa_freq = toa_freq or hdr.fch1
+        self.nchans = nchans or hdr.nchans
+        self.sub_hdr = hdr.new_header({"fch1": self.toa_freq, "nchans": self.nchans})
+        self._disp_delay = int(np.max(np.abs(np.atleast_1d(
+            self.sub_hdr.get_dmdelays(self.pulse_dm, in_samples=True))))) + self.pulse_width * 5
+
+    @property
+    def t_decimate(self) -> int:
+        return max(1, self.pulse_width // 2)
+
+    @property
+    def disp_delay(self) -> int:
+        return self._disp_delay
+
+    @property
+    def block_delay(self) -> int:
+        return ((self.disp_delay // self.t_decimate) + 1) * self.t_decimate
+
+    @property
+    def nsamps(self) -> int:
+        return max(2 * self.block_delay, self.min_nsamps * self.t_decimate)
+
+    @property
+    def nstart(self) -> int:
+        return self.pulse_toa - self.nsamps // 2
+
+    @property
+    def nstart_file(self) -> int:
+        return max(0, self.nstart)
+
+    @property
+    def nsamps_file(self) -> int:
+        return min(self.nsamps + min(0, self.nstart), self.sub_hdr.nsamples - max(0, self.nstart))
+
+    @property
+    def pulse_toa_block(self) -> int:
+        return self.pulse_toa - self.nstart
+
+    def get_data(self, pad_mode: str = "median") -> FilterbankBlock:
+        fil = FilReader(self.filfile)
+        block = fil.read_block(start=self.nstart_file, nsamps=self.nsamps_file,
+                               fch1=self.toa_freq, nchans=self.nchans)
+        if self.nstart < 0 or self.nstart + self.nsamps > self.sub_hdr.nsamples:
+            offset = abs(min(0, self.nstart))
+            block = block.pad_samples(self.nsamps, offset, pad_mode=pad_mode)
+        return block
