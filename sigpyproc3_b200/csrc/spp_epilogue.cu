@@ -147,7 +147,7 @@ __global__ void k_subband(const void* __restrict__ in, int64_t nchans, int64_t n
 // chunk's sum and second central moment.  Final pass merges chunks (Chan et
 // al. 1979 pairwise variance) and forms (best - w*mean) / (std*sqrt(w)).
 // ---------------------------------------------------------------------------
-constexpr int kSnrChunk = 8192;     // downsampled samples per CTA (32 per thread)
+constexpr int kSnrChunk = 6144;     // downsampled samples per CTA (24 per thread)
 constexpr int kSnrThreads = 256;
 constexpr int kSnrMaxW = 4096;
 constexpr int kSnrMaxWidths = 32;
