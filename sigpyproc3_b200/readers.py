@@ -277,12 +277,7 @@ class Filterbank:
         chan_delays = np.atleast_1d(h.get_dmdelays(dm)).astype(np.int32)
         max_delay = int(chan_delays.max())
         gulp = max(2 * max_delay, gulp)
-        # subband of each channel as the reference assigns it: ichan // (nchans / nsubs)
-        factor2 = h.nchans / nbands
-        band = np.array([int(c // factor2) for c in range(h.nchans)], dtype=np.int64)
-        if np.any(np.diff(band) < 0) or band.min() < 0 or band.max() >= nbands:
-            raise ValueError("subband assignment out of range")
-        band_start = np.searchsorted(band, np.arange(nbands + 1)).astype(np.int32)
+        band_start = fold_band_start(h.nchans, nbands)
         dev = torch.device("cuda", torch.cuda.current_device())
         cells = nbins * nints * nbands
         fold_ar = torch.zeros(cells, dtype=torch.float32, device=dev)
@@ -307,6 +302,17 @@ class Filterbank:
         with np.errstate(divide="ignore", invalid="ignore"):
             f /= c
         return FoldedData(f.reshape(nints, nbands, nbins), h.new_header(), period, dm, accel)
+
+
+def fold_band_start(nchans: int, nbands: int) -> np.ndarray:
+    """First channel of each of ``nbands`` subbands (plus ``nchans`` at the end),
+    as kernels.fold assigns channels: ``ichan // (nchans / nbands)`` with
+    Python's float floor division (core/kernels.py:424, :439)."""
+    factor2 = nchans / nbands
+    band = np.array([int(c // factor2) for c in range(nchans)], dtype=np.int64)
+    if np.any(np.diff(band) < 0) or band.min() < 0 or band.max() >= nbands:
+        raise ValueError("subband assignment out of range")
+    return np.searchsorted(band, np.arange(nbands + 1)).astype(np.int32)
 
 
 class FilReader(Filterbank):

@@ -152,3 +152,40 @@ def test_abi_argument_errors_without_gpu():
     assert lib.spp_dedisperse_workspace_bytes(8, 64, 4096, 0, 100) > 64 * 4096
     # nchans * nbits not a multiple of 8
     assert lib.spp_dedisperse_workspace_bytes(2, 3, 4096, 0, 10) == -1
+
+
+@pytest.mark.parametrize("nchans,nbands", [(64, 8), (64, 5), (64, 6), (64, 7), (1000, 32),
+                                           (4096, 30), (17, 17), (31, 4)])
+def test_fold_band_start_matches_reference_assignment(orc, nchans, nbands):
+    """Subband boundaries used by Filterbank.fold equal kernels.fold's
+    ``ichan // (nchans / nsubs)``, here through the oracle's floor division."""
+    from sigpyproc3_b200.readers import fold_band_start
+
+    bs = fold_band_start(nchans, nbands)
+    factor2 = nchans / nbands
+    band = [int(orc.lib().orc_py_floordiv(float(c), factor2)) for c in range(nchans)]
+    assert bs[0] == 0 and bs[-1] == nchans and len(bs) == nbands + 1
+    for b in range(nbands):
+        assert all(band[c] == b for c in range(bs[b], bs[b + 1]))
+
+
+def test_pulse_extractor_window(tmp_path):
+    """PulseExtractor's window arithmetic (readers.py:393-455), restated."""
+    from sigpyproc3_b200 import Header
+    from sigpyproc3_b200.readers import PulseExtractor
+
+    h = Header(nchans=64, fch1=1510.0, foff=-1.0, tsamp=320e-6, nbits=8, nsamples=6000)
+    path = tmp_path / "p.fil"
+    h.write_sigproc(path, np.zeros(6000 * 64, np.uint8))
+    for toa, width, dm, toa_freq, nch in ((3000, 8, 30.0, None, None), (40, 3, 10.0, 1480.0, 16),
+                                          (5990, 1, 50.0, None, 32)):
+        pe = PulseExtractor(str(path), toa, width, dm, min_nsamps=64, toa_freq=toa_freq,
+                            nchans=nch)
+        f1 = toa_freq or 1510.0
+        sub = h.new_header({"fch1": f1, "nchans": nch or 64})
+        disp = int(np.max(np.abs(np.atleast_1d(sub.get_dmdelays(dm))))) + 5 * width
+        tdec = max(1, width // 2)
+        n = max(2 * (((disp // tdec) + 1) * tdec), 64 * tdec)
+        assert (pe.disp_delay, pe.t_decimate, pe.nsamps) == (disp, tdec, n)
+        assert pe.nstart == toa - n // 2 and pe.nstart_file == max(0, toa - n // 2)
+        assert pe.nsamps_file == min(n + min(0, pe.nstart), 6000 - max(0, pe.nstart))
