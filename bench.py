@@ -6,12 +6,14 @@ that fits one GPU): fused unpack + brute-force DM-time transform of a 2-bit
 filterbank, 4096 channels x 2**20 samples (tsamp 64 us, fch1 1500 MHz, foff
 -0.0732421875 MHz), 1024 DM trials on the dmt_transform(1000, 1024) grid
 (0-2000 pc/cm^3), exact int32 output of nsamps - max delay samples.  Seeded
-synthetic data generated on the device (uniform 2-bit samples + three pulses),
-bit-identical to the host twin in sigpyproc3_b200/synth.py.
+synthetic data generated on the device (uniform 2-bit samples + three pulses).
 
 One step = one DMTPlan.execute (corner turn + DM-time kernel) over the whole
 input already resident in HBM.  The input (1 GiB) and output (4.2 GB) exceed
-L2, so no flush is needed between steps.
+L2, so no flush is needed between steps.  The same line carries the
+end-to-end rate through the C ABI from pinned host memory (``e2e``), a
+bit-exact check of whole rows of that end-to-end output against the CPU oracle
+(``parity``), the CPU baseline, and secondary blocks for configs 1 and 3.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -19,8 +21,9 @@ Under torchrun each rank runs an independent replica of the workload (the
 path shards without any exchange); the timed region is bracketed by a
 barrier and device synchronisation, and the elapsed time is the maximum over
 ranks.  --impl reference times the CPU restatement of the reference loop
-(oracle/, the reference itself is Python/numba and is not installed on the
-GPU host) on a bounded sample of the same workload, on rank 0 only.
+(oracle/: the reference is Python + numba, whose source does not travel to
+the GPU host) on a bounded sample of the same workload, on rank 0 only; that
+arm imports neither torch nor this repository's CUDA library.
 """
 
 from __future__ import annotations
@@ -147,23 +150,25 @@ def _workload(args=None):
     return g, dms, delays
 
 
-def cpu_sample_run(g, delays, raw_host: np.ndarray, threads: int, ndm_s: int = 64,
-                   window: int = 65536) -> dict:
-    """Time the CPU loop of the reference (oracle restatement) on a bounded sample:
-    `ndm_s` DM trials spread over the grid, `window` output samples."""
+def cpu_sample_run(nchans: int, nbits: int, delays: np.ndarray, raw_host: np.ndarray,
+                   threads: int, ndm_s: int = 64, window: int = 65536) -> dict:
+    """Time the CPU loop of the reference (oracle restatement of
+    kernels.dedisperse_par: sample-outer, channel-inner float64 sums, rows over
+    all host threads) on a bounded sample: `ndm_s` DM trials spread over the
+    grid, `window` output samples, after unpacking the packed bytes."""
     from oracle import oracle as orc
 
     orc.build()
     orc.set_threads(threads)
     maxd = int(delays.max())
     rows = window + maxd
-    rb = g.nchans * g.nbits // 8
+    rb = nchans * nbits // 8
     packed = raw_host[: rows * rb]
     t0 = time.perf_counter()
-    un = orc.unpack(packed, g.nbits, "big")
+    un = orc.unpack(packed, nbits, "big")
     t1 = time.perf_counter()
     sel = delays[np.linspace(0, delays.shape[0] - 1, ndm_s).astype(int)]
-    orc.dmt_rowmajor(un, sel, g.nchans, rows, window)
+    orc.dmt_rowmajor(un, sel, nchans, rows, window)
     t2 = time.perf_counter()
     # the unpack is shared by all DMs; charge it pro rata to the sample's DMs
     unpack_share = (t1 - t0) * (ndm_s / delays.shape[0])
@@ -172,21 +177,24 @@ def cpu_sample_run(g, delays, raw_host: np.ndarray, threads: int, ndm_s: int = 6
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU loop on the box's host cores, rank 0 only.
+    Inputs come from the oracle's numpy twin of the device generator."""
     if rank != 0:
         return
-    g, dms, delays = _workload()
-    from sigpyproc3_b200 import synth
+    from oracle import synth_host as sh
 
+    delays = sh.c2_delays(sh.dm_grid(1000.0, 1024))
     rows = 65536 + int(delays.max())
-    rb = g.nchans * g.nbits // 8
-    raw_host = synth.c2_filterbank_host(0, rows).ravel()
+    raw_host = sh.c2_filterbank_host(0, rows).ravel()
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_sample_run(g, delays, raw_host, threads, ndm_s=8, window=8192)
+        cpu_sample_run(sh.C2_NCHANS, sh.C2_NBITS, delays, raw_host, threads, ndm_s=8,
+                       window=8192)
     vals = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        vals.append(cpu_sample_run(g, delays, raw_host, threads, ndm_s=256)["value"])
+        vals.append(cpu_sample_run(sh.C2_NCHANS, sh.C2_NBITS, delays, raw_host, threads,
+                                   ndm_s=256)["value"])
     wall = time.perf_counter() - t0
     value = float(statistics.mean(vals))
     sample = "256 of 1024 DM trials (evenly spaced) x 65536 output samples per step, full 4096 channels"
@@ -194,7 +202,7 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8->int32",
-        "data": "synthetic (seeded, host twin of the device generator)",
+        "data": "synthetic (seeded, numpy twin of the device generator)",
         "config": {"workload": WORKLOAD, "rows_in_sample": rows},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
@@ -203,11 +211,29 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def e2e_parity(nchans: int, nbits: int, nsamps: int, delays: np.ndarray, host_in: np.ndarray,
+               host_out: np.ndarray, nvalid: int, rows: np.ndarray) -> dict:
+    """Whole rows of the end-to-end output against the oracle's row-wise
+    restatement of kernels.dedisperse (exact integer sums)."""
+    from oracle import oracle as orc
+
+    t0 = time.perf_counter()
+    orc.build()
+    orc.set_threads(os.cpu_count() or 1)
+    un = orc.unpack(host_in[: nsamps * nchans * nbits // 8], nbits, "big")
+    expect = orc.dmt(un, delays[rows], nchans, nsamps, nvalid)
+    got = host_out[rows, :nvalid]
+    mism = int(np.count_nonzero(got != expect))
+    return {"rows": [int(r) for r in rows], "samples_per_row": int(nvalid), "mismatches": mism,
+            "checked_against": "oracle (row-wise kernels.dedisperse restatement)",
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
 def run_gpu(args, rank, world, local):
     import torch
 
     from sigpyproc3_b200 import synth
-    from sigpyproc3_b200.dedisp import DMTPlan, workspace
+    from sigpyproc3_b200.dedisp import DMTPlan, status_check, status_clear, workspace
 
     g, dms, delays = _workload(args)
     dev = torch.device("cuda", local)
@@ -221,6 +247,7 @@ def run_gpu(args, rank, world, local):
     else:
         tune = plan.autotune(raw, g.nsamps, out, reps=1, cache=os.environ.get("SPP_TUNE_CACHE"))
     ws = workspace(plan.workspace_bytes(g.nsamps), dev)
+    status_clear(ws)
     for _ in range(args.warmup):
         plan.execute(raw, g.nsamps, out, ws=ws)
     torch.cuda.synchronize()
@@ -239,6 +266,7 @@ def run_gpu(args, rank, world, local):
     torch.cuda.synchronize()
     _barrier(world)
     clk = clocks.stop()
+    status_check(ws)  # raises if any launch flagged a device error (outside the timing)
     ms = e0.elapsed_time(e1)
     tk = plan.timing_read()
     plan.timing(False)
@@ -273,6 +301,7 @@ def run_gpu(args, rank, world, local):
     # end to end through the C ABI from pinned host buffers
     e2e = None
     cpu = None
+    parity = None
     if rank == 0 and not args.no_e2e:
         host_in = torch.empty(raw.numel(), dtype=torch.uint8).pin_memory()
         host_in.copy_(raw.cpu())
@@ -294,15 +323,46 @@ def run_gpu(args, rank, world, local):
         e2e = {"value": delays.shape[0] * nvalid / ((t1 - t0) / ne), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(delays.shape[0] * nvalid * 4),
                "steps": ne, "path": "spp_dmt_execute_host (C ABI), pinned host buffers"}
-        # spot-check the e2e output against the device result (first row)
+        # whole rows of the end-to-end output against the oracle (outside timing)
+        if not args.no_parity:
+            prow = np.unique(np.linspace(0, delays.shape[0] - 1, 8).astype(int))
+            parity = e2e_parity(g.nchans, g.nbits, g.nsamps, delays, host_in.numpy(),
+                                host_out.numpy(), nvalid, prow)
         if world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
             rows = 65536 + int(delays.max())
             rb = g.nchans * g.nbits // 8
-            c = cpu_sample_run(g, delays, host_in.numpy()[: rows * rb], threads, ndm_s=256)
+            c = cpu_sample_run(g.nchans, g.nbits, delays, host_in.numpy()[: rows * rb], threads,
+                               ndm_s=256)
             cpu = {"value": c["value"], "unit": UNIT, "cores": threads, "kind": "port",
                    "sample": f"{c['ndm']} of 1024 DM trials x {c['window']} output samples, "
                              f"{c['seconds']:.1f} s of CPU time"}
+        del host_in, host_out, hws
+    tile = plan.describe()
+    plan.close()
+    del raw
+    torch.cuda.empty_cache()
+    # secondary workloads on the same GPU, after the headline (rank 0 of one GPU)
+    secondary = {}
+    if rank == 0 and world == 1 and not args.no_secondary:
+        from sigpyproc3_b200 import workloads
+
+        c1 = workloads.measure_c1(max(1, min(args.steps, 5)))
+        secondary["config1"] = {
+            "metric": c1["metric"], "value": c1["value"], "unit": UNIT,
+            "us_per_call": c1["ms_per_step"] * 1e3, "roofline_frac": c1["roofline"]["frac"],
+            "achieved_gbs": c1["roofline"]["achieved"], "peak_gbs": c1["roofline"]["peak"],
+            "long_block_frac": c1["long_block"]["frac"], "e2e": c1["e2e"],
+            "timing": "CUDA-graph replay of 16 calls over rotating L2-cold inputs"}
+        torch.cuda.empty_cache()
+        c3 = workloads.measure_c3(steps=max(1, min(args.steps, 2)), warmup=1, beams=64, batch=4,
+                                  rank=0, world=1)
+        secondary["config3"] = {
+            "metric": c3["metric"], "value": c3["value"], "unit": UNIT,
+            "plain_per_call": c3["plain_per_call"]["value"],
+            "served_over_plain": c3["served_over_plain"], "beams": 64,
+            "ms_per_step": c3["ms_per_step"], "steps": c3["steps"]}
+        torch.cuda.empty_cache()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -313,139 +373,16 @@ def run_gpu(args, rank, world, local):
                        f"REDUCED profiling case ndm={args.ndm} nsamps={args.nsamps}",
                        "l2": "inputs larger than L2 (1 GiB in, 4.2 GB out)",
                        "ndm": int(delays.shape[0]), "nvalid": int(nvalid),
-                       "tile": plan.describe(), "autotune_ms": tune.get("all_ms"),
+                       "tile": tile, "autotune_ms": tune.get("all_ms"),
                        "parallelism": f"replicas x{world}"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": 2 * args.steps, "clocks": clk,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "parity": parity,
+            "gpu_launches": 2 * args.steps, "clocks": clk, "secondary": secondary,
         }
         print(json.dumps(line), flush=True)
-    plan.close()
 
 
 def _line(**kw):
     print(json.dumps(kw), flush=True)
-
-
-def run_c3(args, rank, world, local):
-    """Config 3: 64 beams of uneven length, two-stage subband search (32
-    subbands, 512 trials 0-1000), downsample 1/2/4, boxcar widths 1..256 ->
-    S/N peaks; each batch of beams is one CUDA graph of persistent launches.
-    Also times the plain per-call path (one brute-force dedispersion + S/N per
-    beam and DM) on a subset."""
-    import torch
-
-    from sigpyproc3_b200 import Header, multi, synth
-    from sigpyproc3_b200.dedisp import dedisperse_block
-    from sigpyproc3_b200.search import boxcar_snr
-    from sigpyproc3_b200.subband import SubbandPlan, SubbandSearch
-
-    g = synth.C3
-    h = Header(nchans=g.nchans, fch1=g.fch1, foff=g.foff, tsamp=g.tsamp, nbits=8)
-    plan = SubbandPlan(h, synth.dm_grid(500.0, 512), nsub=32, group=16)
-    rng = np.random.default_rng(3)
-    nbeams = args.beams
-    lens = rng.integers(1 << 18, (1 << 21) + 1, size=nbeams)
-    lo, hi = multi.shard_range(nbeams, rank, world)
-    th = synth.gauss_u8_thresholds(96.0, 12.0)
-    factors, widths = (1, 2, 4), tuple(1 << k for k in range(9))
-    batch = args.batch
-    # autotune the two stages on the first batch
-    tune_lens = lens[lo:lo + batch]
-    best, best_ms = (0, 0), None
-    for v1, v2 in ((0, 0), (1, 0), (2, 0), (3, 0)):
-        srch = SubbandSearch(plan, tune_lens, factors=factors, widths=widths, variants=(v1, v2))
-        for b in srch.beams:
-            synth.gauss_u8_device(b.raw.numel(), 99, 96.0, 12.0, out=b.raw)
-        srch.run()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        srch.run(snr=False)
-        e1.record()
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        if best_ms is None or ms < best_ms:
-            best, best_ms = (v1, v2), ms
-        del srch
-        torch.cuda.empty_cache()
-    v1 = best[0]
-    best_ms = None
-    for v2 in range(4):
-        srch = SubbandSearch(plan, tune_lens, factors=factors, widths=widths, variants=(v1, v2))
-        for b in srch.beams:
-            synth.gauss_u8_device(b.raw.numel(), 99, 96.0, 12.0, out=b.raw)
-        srch.run()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        srch.run(snr=False)
-        e1.record()
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        if best_ms is None or ms < best_ms:
-            best, best_ms = (v1, v2), ms
-        del srch
-        torch.cuda.empty_cache()
-    total_ms, units = 0.0, 0
-    peaks = []
-    torch.cuda.synchronize()
-    _barrier(world)
-    for b0 in range(lo, hi, batch):
-        blens = lens[b0:min(hi, b0 + batch)]
-        srch = SubbandSearch(plan, blens, factors=factors, widths=widths, variants=best)
-        for i, b in enumerate(srch.beams):
-            synth.gauss_u8_device(b.raw.numel(), 3000 + b0 + i, 96.0, 12.0, out=b.raw)
-        srch.capture()
-        for _ in range(args.warmup):
-            srch.replay()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(args.steps):
-            srch.replay()
-        e1.record()
-        e1.synchronize()
-        total_ms += e0.elapsed_time(e1) / args.steps
-        units += sum(512 * b.nvalid for b in srch.beams)
-        peaks += [float(b.snr.max()) for b in srch.beams]
-        assert srch.status_ok()
-        del srch
-        torch.cuda.empty_cache()
-    ms_max = multi.max_over_ranks(total_ms)
-    units_all = multi.sum_over_ranks(units)
-    value = units_all / (ms_max / 1e3)
-    # plain per-call path on a subset: 2 beams x 16 DMs, brute force + S/N per call
-    nsub_beams, nsub_dms = 2, 16
-    dms = plan.dms[np.linspace(0, 511, nsub_dms).astype(int)]
-    t_plain, u_plain = 0.0, 0
-    for bi in range(nsub_beams):
-        n = int(lens[bi])
-        raw = synth.gauss_u8_device(n * g.nchans, 3000 + bi, 96.0, 12.0)
-        d_all = np.atleast_2d(h.get_dmdelays(dms)).astype(np.int32)
-        tim = torch.empty(n, dtype=torch.float32, device="cuda")
-        for dmi in range(nsub_dms):  # warm
-            dedisperse_block(raw, d_all[dmi], g.nchans, n, tim)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for dmi in range(nsub_dms):
-            d = d_all[dmi]
-            nvi = dedisperse_block(raw, d, g.nchans, n, tim)
-            boxcar_snr(tim[:nvi].view(1, -1), widths=widths, factors=factors)
-            u_plain += nvi
-        torch.cuda.synchronize()
-        t_plain += time.perf_counter() - t0
-    plain = u_plain / t_plain
-    if rank == 0:
-        _line(metric="DM-trial x samples/s, config 3 (batched two-stage subband search + S/N)",
-              value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
-              ms_per_step=ms_max, higher_is_better=True, scaling="weak", vs_baseline=None,
-              dtype="u8->uint16->int32 (+f32 S/N)", data="synthetic (device generator, seeded)",
-              config={"workload": f"config 3: {nbeams} beams nsamps U[2^18,2^21], 1024 ch 8-bit, "
-                      "32 subbands x 16-trial groups, 512 trials 0-1000, downsample 1/2/4, "
-                      "widths 1..256", "batch_beams": batch, "variants": list(best),
-                      "beams_total_samples": int(lens.sum())},
-              plain_per_call={"value": plain, "unit": UNIT, "path": "dedisperse_block + boxcar_snr "
-                              "per (beam, DM), brute force over 1024 channels",
-                              "sample": f"{nsub_beams} beams x {nsub_dms} DMs"},
-              served_over_plain=value / plain, max_snr=max(peaks) if peaks else None,
-              gpu_launches=None)
 
 
 def main():
@@ -458,6 +395,8 @@ def main():
     ap.add_argument("--e2e-block", type=int, default=65536,
                     help="output samples per host-streaming block in the e2e leg")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the e2e row check")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the config 1/3 blocks")
     ap.add_argument("--variant", type=int, default=None, help="fix the kernel variant")
     ap.add_argument("--workload", choices=["c2", "c3", "c4", "c1", "c5", "snr", "fold"], default="c2")
     ap.add_argument("--beams", type=int, default=64, help="config 3: number of beams")
@@ -474,9 +413,7 @@ def main():
         return
     rank, world, local = _dist_init()
     try:
-        if args.workload == "c3":
-            run_c3(args, rank, world, local)
-        elif args.workload == "c2":
+        if args.workload == "c2":
             run_gpu(args, rank, world, local)
         else:
             from sigpyproc3_b200 import workloads

@@ -149,6 +149,15 @@ int spp_dedisperse_noalloc(const void* in, int nbits, int bitorder, int64_t ncha
                            int64_t nsamps, const int32_t* delays, int32_t delay_min,
                            int32_t delay_max, float* out, int64_t out_len,
                            int64_t out_start, int acc, void* stream);
+/* The device status words of the last spp_dedisperse_noalloc call on the
+ * current device (they live in the fixed array, which the caller cannot
+ * address): copies the 4 words to host_out[4], synchronising `stream`, and
+ * returns SPP_ERR_DEVICE if word 0 is non-zero -- a bounded wait ran out
+ * (SPP_DEV_TIMEOUT, the output is incomplete) or a delay lay outside the
+ * declared [delay_min, delay_max] and was clamped (SPP_DEV_RANGE, the output
+ * is wrong).  Each spp_dedisperse_noalloc call clears the words first.  No
+ * counterpart in the reference. */
+int spp_dedisperse_noalloc_status_read(uint32_t* host_out, void* stream);
 
 /* ---- R3: DM-trial batch (DM-time transform) -----------------------------------
  * Replaces FilterbankBlock.dmt_transform (block.py:309-343) / kernels.dmt_block

@@ -29,12 +29,15 @@ import tempfile
 import types
 from pathlib import Path
 
-REF_ROOT = Path(os.environ.get("SPP_REFERENCE_ROOT", "/root/reference"))
+# the reference source tree, named by the caller; unset means "not available"
+_ROOT_ENV = os.environ.get("SPP_REFERENCE_ROOT", "")
+REF_ROOT = Path(_ROOT_ENV)
 SRC = REF_ROOT / "src" / "sigpyproc"
+TEST_DATA = REF_ROOT / "tests" / "data"
 
 
 def available() -> bool:
-    return (SRC / "core" / "kernels.py").is_file()
+    return bool(_ROOT_ENV) and (SRC / "core" / "kernels.py").is_file()
 
 
 def load_kernels():

@@ -36,6 +36,7 @@ int orc_max_threads(void) {
 void orc_unpack(const uint8_t* in, int64_t nbytes, int nbits, int big, uint8_t* out) {
   const int per = 8 / nbits;
   const unsigned mask = (1u << nbits) - 1u;
+#pragma omp parallel for schedule(static) num_threads(g_threads)
   for (int64_t i = 0; i < nbytes; ++i) {
     const unsigned b = in[i];
     for (int k = 0; k < per; ++k) {
@@ -84,28 +85,53 @@ int64_t orc_dedisperse_f32(const float* in, float* out, const int32_t* delays, i
   return nvalid > 0 ? nvalid : 0;
 }
 
+/* Channel-major copy of a time-major block (cm[c][r] = in[r][c]), so the
+ * per-channel loops below read contiguously.  Changes no arithmetic. */
+static void *to_channel_major(const void *in, int64_t nchans, int64_t nsamps, size_t esz) {
+  void *cm = malloc((size_t)(nchans * nsamps) * esz + 1);
+  if (!cm) return NULL;
+#pragma omp parallel for schedule(static) num_threads(g_threads)
+  for (int64_t c = 0; c < nchans; ++c) {
+    if (esz == 1) {
+      const uint8_t *src = (const uint8_t *)in + c;
+      uint8_t *dst = (uint8_t *)cm + c * nsamps;
+      for (int64_t r = 0; r < nsamps; ++r) dst[r] = src[r * nchans];
+    } else {
+      const float *src = (const float *)in + c;
+      float *dst = (float *)cm + c * nsamps;
+      for (int64_t r = 0; r < nsamps; ++r) dst[r] = src[r * nchans];
+    }
+  }
+  return cm;
+}
+
 /* DM-trial batch, row-wise R2 contract: out[i][t] = dedisperse(x, D[i])[t]
  * for t < nvalid (= nsamps - max over all |D|), uint8 input, exact int32
  * sums.  Parallel over DM rows. */
 void orc_dmt_u8_i32(const uint8_t* in, const int32_t* delays, int64_t ndm, int64_t nchans,
                     int64_t nsamps, int64_t nvalid, int32_t* out, int64_t out_stride) {
+  uint8_t *cm = (uint8_t *)to_channel_major(in, nchans, nsamps, 1);
+  if (!cm) abort();
 #pragma omp parallel for schedule(dynamic, 1) num_threads(g_threads)
   for (int64_t i = 0; i < ndm; ++i) {
     const int32_t* d = delays + i * nchans;
     int32_t* o = out + i * out_stride;
     for (int64_t t = 0; t < nvalid; ++t) o[t] = 0;
     for (int64_t c = 0; c < nchans; ++c) {
-      const uint8_t* col = in + c;
+      const uint8_t* row = cm + c * nsamps;
       const int64_t dc = d[c];
-      for (int64_t t = 0; t < nvalid; ++t) o[t] += col[wrap_neg(t + dc, nsamps) * nchans];
+      for (int64_t t = 0; t < nvalid; ++t) o[t] += row[wrap_neg(t + dc, nsamps)];
     }
   }
+  free(cm);
 }
 
 /* Float32 input: float64 sum per output in channel order, stored float32
  * (and optionally float64 in out64). */
 void orc_dmt_f32(const float* in, const int32_t* delays, int64_t ndm, int64_t nchans,
                  int64_t nsamps, int64_t nvalid, float* out, double* out64, int64_t out_stride) {
+  float *cm = (float *)to_channel_major(in, nchans, nsamps, 4);
+  if (!cm) abort();
 #pragma omp parallel num_threads(g_threads)
   {
     double* acc = (double*)malloc(sizeof(double) * (nvalid > 0 ? nvalid : 1));
@@ -114,9 +140,9 @@ void orc_dmt_f32(const float* in, const int32_t* delays, int64_t ndm, int64_t nc
       const int32_t* d = delays + i * nchans;
       for (int64_t t = 0; t < nvalid; ++t) acc[t] = 0.0;
       for (int64_t c = 0; c < nchans; ++c) {
-        const float* col = in + c;
+        const float* row = cm + c * nsamps;
         const int64_t dc = d[c];
-        for (int64_t t = 0; t < nvalid; ++t) acc[t] += (double)col[wrap_neg(t + dc, nsamps) * nchans];
+        for (int64_t t = 0; t < nvalid; ++t) acc[t] += (double)row[wrap_neg(t + dc, nsamps)];
       }
       for (int64_t t = 0; t < nvalid; ++t) {
         if (out) out[i * out_stride + t] = (float)acc[t];
@@ -125,6 +151,7 @@ void orc_dmt_f32(const float* in, const int32_t* delays, int64_t ndm, int64_t nc
     }
     free(acc);
   }
+  free(cm);
 }
 
 /* kernels.dmt_block (core/kernels.py:1155-1168) semantics on time-major

@@ -45,13 +45,31 @@ def _stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
+    """Compile each .cu to an object in parallel (no device code crosses files),
+    then link the shared library."""
     if not force and not _stale():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    jobs = []
+    for src in sources():
+        obj = objdir / (src.stem + ".o")
+        jobs.append((obj, [_nvcc(), *compile_flags, *(extra or []), "-c", "-o", str(obj), str(src)]))
+
+    def run(job):
+        if verbose:
+            print(" ".join(job[1]))
+        subprocess.run(job[1], check=True)
+        return job[0]
+
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+        objs = list(ex.map(run, jobs))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [_nvcc(), *NVCC_FLAGS, *(extra or []), "-o", str(tmp), *map(str, sources())]
-    if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+    subprocess.run([_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+                    "-o", str(tmp), *map(str, objs)], check=True)
     tmp.replace(LIB)
     return LIB
 

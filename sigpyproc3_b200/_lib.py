@@ -53,6 +53,7 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_dedisperse_noalloc_max_bytes": ([], _i64),
     "spp_dedisperse_noalloc": ([_p, _int, _int, _i64, _i64, _p, _i32, _i32, _p, _i64, _i64, _int,
                                 _p], _int),
+    "spp_dedisperse_noalloc_status_read": ([_p, _p], _int),
     "spp_dmt_plan_create": ([ctypes.POINTER(_p), _int, _int, _i64, _i64, _i64, _p, _int, _int,
                              _int], _int),
     "spp_dmt_plan_destroy": ([_p], _int),

@@ -528,6 +528,17 @@ int spp_dedisperse_noalloc(const void* in, int nbits, int bitorder, int64_t ncha
   return launch_dmt(*v, a, g.ntiles_t, 1, st);
 }
 
+// The status words of the last spp_dedisperse_noalloc call on the current
+// device sit at the head of the fixed array, where the caller has no pointer
+// to them; this copies them out (synchronising `stream`).
+int spp_dedisperse_noalloc_status_read(uint32_t* host_out, void* stream) {
+  if (!host_out) return fail(SPP_ERR_ARG, "spp_dedisperse_noalloc_status_read: null pointer");
+  void* base = nullptr;
+  const int rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  return spp_status_read(base, host_out, stream);
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -881,6 +892,12 @@ int spp_dmt_execute_host(const spp_dmt_plan* p, const void* in_host, int64_t nsa
   const int64_t rb = host_row_bytes(p);
   const int64_t es = 4;
   const int64_t nblocks = ceil_div(nvalid, block_nsamps);
+  // each buffer set's run workspace starts with the device status words of
+  // the kernels it hosts: cleared here, read back once everything finished
+  for (int k = 0; k < kHostSets && rc == SPP_OK; ++k)
+    rc = cuda_status(cudaMemsetAsync(ws + kStatusBytes + k * h.set_bytes + h.in_bytes + h.out_bytes,
+                                     0, 16, s[k]),
+                     "status clear");
   for (int64_t b = 0; b < nblocks && rc == SPP_OK; ++b) {
     const int k = (int)(b % kHostSets);
     uint8_t* set = ws + kStatusBytes + k * h.set_bytes;
@@ -903,6 +920,15 @@ int spp_dmt_execute_host(const spp_dmt_plan* p, const void* in_host, int64_t nsa
     int r2 = cuda_status(cudaStreamSynchronize(s[i]), "stream sync");
     if (!rc) rc = r2;
     cudaStreamDestroy(s[i]);
+  }
+  for (int k = 0; k < kHostSets && rc == SPP_OK; ++k) {
+    uint32_t words[4] = {0, 0, 0, 0};
+    rc = cuda_status(cudaMemcpy(words, ws + kStatusBytes + k * h.set_bytes + h.in_bytes + h.out_bytes,
+                                16, cudaMemcpyDeviceToHost),
+                     "status copy");
+    if (rc == SPP_OK && words[0] != 0)
+      rc = fail(SPP_ERR_DEVICE, "device status 0x%x (block %u, detail 0x%x)", words[0], words[1],
+                words[2]);
   }
   return rc;
 }

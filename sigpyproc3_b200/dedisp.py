@@ -47,6 +47,26 @@ def workspace(nbytes: int, device: torch.device | int | None = None,
     return buf
 
 
+def status_clear(ws: torch.Tensor, stream: torch.cuda.Stream | None = None) -> None:
+    """Zero the device status block at the head of a workspace (stream-ordered).
+
+    Kernels that wait on an mbarrier with a time limit, or that clamp a delay
+    outside the declared range, record it in these words instead of faulting;
+    a fresh workspace holds arbitrary bytes, so clear it before the calls whose
+    status is to be read."""
+    _lib.check(_lib.load().spp_status_clear(ws.data_ptr(), stream_handle(stream, ws.device)))
+
+
+def status_check(ws: torch.Tensor, stream: torch.cuda.Stream | None = None) -> None:
+    """Synchronise ``stream`` and raise :class:`SppError` (SPP_ERR_DEVICE) if any
+    call since the last :func:`status_clear` on this workspace flagged a device
+    error: a bounded wait that ran out (the output is incomplete) or a delay
+    clamped into the declared range (the output is wrong)."""
+    words = np.zeros(4, dtype=np.uint32)
+    _lib.check(_lib.load().spp_status_read(ws.data_ptr(), words.ctypes.data,
+                                           stream_handle(stream, ws.device)))
+
+
 def _as_raw(data) -> torch.Tensor:
     if not torch.is_tensor(data):
         raise TypeError("expected a torch tensor")
@@ -232,7 +252,11 @@ class DMTPlan:
     # -- execution --
     def execute(self, raw: torch.Tensor, nsamps: int | None = None, out: torch.Tensor | None = None,
                 out_start: int = 0, stream: torch.cuda.Stream | None = None,
-                ws: torch.Tensor | None = None) -> torch.Tensor:
+                ws: torch.Tensor | None = None, check: bool = False) -> torch.Tensor:
+        """DM-time array of one block (stream-ordered).  ``check=True`` clears the
+        workspace's device status first and reads it after the launch (a
+        synchronisation), raising SppError if the kernel flagged an error;
+        otherwise read it with :func:`status_check` after a run of calls."""
         raw = _as_raw(raw)
         if nsamps is None:
             rb = self.nchans * 4 if self.nbits == 32 else self.nchans * self.nbits // 8
@@ -243,9 +267,13 @@ class DMTPlan:
         stride = out.stride(0) if out.dim() == 2 else out.numel()
         if ws is None:
             ws = workspace(self.workspace_bytes(nsamps), raw.device, stream)
+        if check:
+            status_clear(ws, stream)
         _lib.check(_lib.load().spp_dmt_execute(
             self._h, raw.data_ptr(), nsamps, out.data_ptr(), stride, out_start, ws.data_ptr(),
             ws.numel(), stream_handle(stream, raw.device)))
+        if check:
+            status_check(ws, stream)
         return out
 
     def execute_zero_dm(self, raw: torch.Tensor, nsamps: int, bpass: torch.Tensor,

@@ -19,7 +19,8 @@ import torch
 
 from . import _lib
 from .block import FilterbankBlock
-from .dedisp import DMTPlan, dedisperse_block, stream_handle, workspace
+from .dedisp import (DMTPlan, dedisperse_block, status_check, status_clear, stream_handle,
+                     workspace)
 from .folded import FoldedData
 from .header import Header
 from .io.bits import bitorder_code
@@ -173,11 +174,19 @@ class Filterbank:
         dev = torch.device("cuda", torch.cuda.current_device())
         tim = torch.zeros(max(tim_len, 0), dtype=torch.float32, device=dev)
         ddev = torch.from_numpy(chan_delays).to(dev)
+        # one workspace for every block (a block never exceeds the gulp); its
+        # device status words collect any kernel-side error over the whole run
+        need = _lib.load().spp_dedisperse_workspace_bytes(
+            h.nbits, h.nchans, min(gulp, h.nsamples), int(chan_delays.min()),
+            int(chan_delays.max()))
+        ws = workspace(max(int(need), 256), dev)
+        status_clear(ws)
         for nsamps_r, ii, raw in self.stream_blocks(gulp, start, nsamps, skipback=max_delay,
                                                     **plan_kwargs):
             dedisperse_block(raw, chan_delays, h.nchans, nsamps_r, tim, ii * (gulp - max_delay),
                              nbits=h.nbits, bitorder=self.bitorder, acc=_lib.ACC_F64,
-                             delays_dev=ddev)
+                             delays_dev=ddev, ws=ws)
+        status_check(ws)
         return TimeSeries(tim, h.new_header({"nchans": 1, "dm": dm, "nsamples": tim_len}))
 
     # --- R3: DM-trial batch ---
@@ -209,9 +218,12 @@ class Filterbank:
         plan = DMTPlan(delays, h.nchans, min(gulp, span), nbits=h.nbits, bitorder=self.bitorder,
                        out_dtype=out_dtype)
         try:
+            ws = workspace(plan.workspace_bytes(min(gulp, span)), dev)
+            status_clear(ws)
             for nsamps_r, ii, raw in self.stream_blocks(gulp, start, nsamps, skipback=max_delay,
                                                         **plan_kwargs):
-                plan.execute(raw, nsamps_r, out, out_start=ii * (gulp - max_delay))
+                plan.execute(raw, nsamps_r, out, out_start=ii * (gulp - max_delay), ws=ws)
+            status_check(ws)
         finally:
             torch.cuda.current_stream(dev).synchronize()
             plan.close()

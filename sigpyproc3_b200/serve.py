@@ -92,6 +92,7 @@ class _Batch:
     bytes: int
     buffers: list = field(default_factory=list)
     worklists: list = field(default_factory=list)
+    status: torch.Tensor | None = None  # pinned host copy of the work lists' status words
 
 
 class Server:
@@ -239,9 +240,14 @@ class Server:
                     c._snr_dev = snr
                     c._snr_host = torch.empty(snr.shape, dtype=torch.float32).pin_memory()
                     c._snr_host.copy_(snr, non_blocking=True)
+            # the work lists' device status words travel back with the batch
+            status_host = torch.empty((max(len(wls), 1), 4), dtype=torch.int32).pin_memory()
+            status_host.zero_()
+            for i, wl in enumerate(wls):
+                status_host[i].copy_(wl.status, non_blocking=True)
         ev = torch.cuda.Event()
         ev.record(stream)
-        self.inflight.append(_Batch(chunks, stream, ev, total, bufs, wls))
+        self.inflight.append(_Batch(chunks, stream, ev, total, bufs, wls, status_host))
         self.in_use += total
         self.batches += 1
 
@@ -250,6 +256,11 @@ class Server:
         keep = []
         for b in self.inflight:
             if b.done.query():
+                if b.status is not None and bool((b.status[:, 0] != 0).any()):
+                    w = b.status[b.status[:, 0] != 0][0].tolist()
+                    raise _lib.SppError(_lib.SPP_ERR_DEVICE,
+                                        f"work-list device status 0x{w[0] & 0xffffffff:x} "
+                                        f"(block {w[1]}, detail 0x{w[2] & 0xffffffff:x})")
                 t = now_fn()
                 for c in b.chunks:
                     c.t_done = t
@@ -329,7 +340,7 @@ def plain_process(beams: dict[int, BeamState] | None, chunk: Chunk, st: BeamStat
         return chunk
     plan = DMTPlan(st.delays, st.nchans, rows, nbits=st.nbits,
                    bitorder="little" if st.nbits == 1 else "big", out_dtype=torch.int32)
-    dmt = plan.execute(raw[start_row * st.row_bytes:], rows - start_row)
+    dmt = plan.execute(raw[start_row * st.row_bytes:], rows - start_row, check=True)
     assert dmt.shape[1] == chunk.nvalid
     if chunk.nvalid > 0:
         snr, _ = boxcar_snr(dmt, widths=widths, factors=(1,), with_index=False)

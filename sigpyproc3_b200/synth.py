@@ -5,10 +5,10 @@ No public dataset is involved: every input is generated here from a seed.
 * Small (CPU-sized) inputs use ``numpy.random.default_rng(seed)``.
 * Large inputs are generated on the GPU with a counter-based hash (the
   SplitMix64 finaliser of Steele, Lea & Flood 2014 applied to
-  ``seed * 2**40 + index``).  Integer outputs (uniform bits, Gaussian-shaped
-  uint8 via a 256-entry CDF threshold table built here in float64) are
-  bit-identical between :func:`hash_u64` (numpy) and the device generator, so
-  tests can regenerate any slice on the host.
+  ``seed << 40 ^ index``): uniform bytes, or Gaussian-shaped uint8 through a
+  256-entry CDF threshold table built here in float64.  The integer outputs
+  are a pure function of (seed, index), so the test suite's numpy twins of
+  these generators regenerate any slice on the host byte for byte.
 """
 
 from __future__ import annotations
@@ -20,18 +20,6 @@ import numpy as np
 
 from . import params
 
-MASK64 = (1 << 64) - 1
-
-
-def hash_u64(seed: int, index: np.ndarray) -> np.ndarray:
-    """SplitMix64 finaliser of ``seed << 40 ^ index`` (uint64, vectorised)."""
-    with np.errstate(over="ignore"):
-        z = (np.uint64(seed) << np.uint64(40)) ^ index.astype(np.uint64)
-        z = z + np.uint64(0x9E3779B97F4A7C15)
-        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-        return z ^ (z >> np.uint64(31))
-
 
 def gauss_u8_thresholds(mean: float, std: float) -> np.ndarray:
     """uint32 thresholds T[v] = floor(2**32 * P(round(X) <= v)), X ~ N(mean, std),
@@ -41,21 +29,6 @@ def gauss_u8_thresholds(mean: float, std: float) -> np.ndarray:
         p = 0.5 * (1.0 + math.erf((v + 0.5 - mean) / (std * math.sqrt(2.0))))
         t[v] = min(int(p * 2**32), 2**32 - 1)
     return t.astype(np.uint32)
-
-
-def gauss_u8_host(seed: int, start: int, count: int, thresholds: np.ndarray) -> np.ndarray:
-    """Host twin of the device Gaussian-uint8 generator for bytes [start, start+count)."""
-    u = (hash_u64(seed, np.arange(start, start + count, dtype=np.uint64)) >> np.uint64(32)).astype(
-        np.uint32
-    )
-    return np.searchsorted(thresholds, u, side="right").astype(np.uint8)
-
-
-def uniform_bytes_host(seed: int, start: int, count: int) -> np.ndarray:
-    """Host twin of the device uniform-byte generator."""
-    return (hash_u64(seed, np.arange(start, start + count, dtype=np.uint64)) & np.uint64(0xFF)).astype(
-        np.uint8
-    )
 
 
 # ---------------------------------------------------------------------------
@@ -118,28 +91,6 @@ def c2_pulse_rows(g: Geometry = C2) -> list[np.ndarray]:
     return [(t + g.delays(dm)).astype(np.int64) - C2_PULSE_WIDTH // 2 for dm, t in C2_PULSES]
 
 
-def c2_filterbank_host(start_row: int, nrows: int, g: Geometry = C2, seed: int = 2) -> np.ndarray:
-    """Host twin of the device config-2 generator for rows [start_row, start_row+nrows):
-    uniform 2-bit samples plus the three pulses (+1 level, saturating at 3).
-    Returns packed big-endian bytes (nrows, nchans/4)."""
-    rb = g.nchans * g.nbits // 8
-    raw = uniform_bytes_host(seed, start_row * rb, nrows * rb).reshape(nrows, rb)
-    vals = np.empty((nrows, g.nchans), dtype=np.uint8)
-    for k in range(4):
-        vals[:, k::4] = (raw >> (6 - 2 * k)) & 3
-    for p in c2_pulse_rows(g):
-        for c in range(g.nchans):
-            lo = max(p[c], start_row)
-            hi = min(p[c] + C2_PULSE_WIDTH, start_row + nrows)
-            if lo < hi:
-                sl = vals[lo - start_row : hi - start_row, c]
-                vals[lo - start_row : hi - start_row, c] = np.minimum(sl + 1, 3)
-    out = np.zeros((nrows, rb), dtype=np.uint8)
-    for k in range(4):
-        out |= vals[:, k::4] << (6 - 2 * k)
-    return out
-
-
 # ---------------------------------------------------------------------------
 # Device generators (libsppgpu spp_synth_*)
 # ---------------------------------------------------------------------------
@@ -187,8 +138,8 @@ def gauss_f32_device(n: int, seed: int, mean: float = 0.0, std: float = 1.0, sta
 
 
 def c2_filterbank_device(g: Geometry = C2, seed: int = 2, stream=None):
-    """Config 2 on the device: uniform 2-bit packed samples + three pulses.
-    Identical bytes to :func:`c2_filterbank_host`."""
+    """Config 2 on the device: uniform 2-bit packed samples + three pulses
+    (+1 level over C2_PULSE_WIDTH samples, saturating at 3)."""
     import torch
 
     from . import _lib

@@ -1,5 +1,7 @@
 """Benchmark workloads other than the default DM-time transform (bench.py
---workload c1|c4|c5).  Each prints one JSON line through ``emit``."""
+--workload c1|c3|c4|c5|snr|fold).  Each prints one JSON line through ``emit``;
+``measure_c1`` and ``measure_c3`` also feed the secondary blocks of the
+default line."""
 
 from __future__ import annotations
 
@@ -19,13 +21,20 @@ def _events():
 
 
 def run(name: str, args, rank: int, world: int, local: int, emit) -> None:
-    {"c1": run_c1, "c4": run_c4, "c5": run_c5, "snr": run_snr,
+    {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "snr": run_snr,
      "fold": run_fold}[name](args, rank, world, local, emit)
 
 
 def run_c1(args, rank, world, local, emit) -> None:
     """Config 1 through the single-DM drop-in kernel (kernels.dedisperse):
     uint8 65536 x 256, DM 100, 16 rotating input copies (272 MB > L2)."""
+    m = measure_c1(max(args.steps, 1))
+    if rank == 0:
+        emit(**m)
+
+
+def measure_c1(steps: int) -> dict:
+    """Config-1 measurements as the fields of one bench line (see run_c1)."""
     import json
     from pathlib import Path
 
@@ -58,7 +67,7 @@ def run_c1(args, rank, world, local, emit) -> None:
         graph.replay()
     torch.cuda.synchronize()
     e0, e1 = _events()
-    reps = max(args.steps, 1) * 4
+    reps = steps * 4
     e0.record()
     for _ in range(reps):
         graph.replay()
@@ -132,9 +141,9 @@ def run_c1(args, rank, world, local, emit) -> None:
     peaks = json.loads((Path(__file__).resolve().parents[1] / "MEASURED_PEAKS.json").read_text()) \
         if (Path(__file__).resolve().parents[1] / "MEASURED_PEAKS.json").exists() else {"hbm_gbs": 6650.0}
     gbs = alg / (ms / 1e3) / 1e9
-    if rank == 0:
-        emit(metric="DM-trial x samples/s, config 1 (single-DM drop-in, 8-bit 256 ch)",
-             value=nv / (ms / 1e3), unit=UNIT, n_gpus=world, steps=reps, warmup=1,
+    del raws, outs, graph
+    return dict(metric="DM-trial x samples/s, config 1 (single-DM drop-in, 8-bit 256 ch)",
+             value=nv / (ms / 1e3), unit=UNIT, n_gpus=1, steps=reps, warmup=1,
              ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
              dtype="u8->f32", data="synthetic (numpy seed 1, injected DM-100 pulse)",
              config={"workload": "config 1: Filterbank.dedisperse(100) kernel path, 16 rotating "
@@ -155,6 +164,130 @@ def run_c1(args, rank, world, local, emit) -> None:
                   "d2h_bytes_per_step": int(nv * 4), "ms_per_call": e2e_s * 1e3,
                   "path": "ArrayFilterbank(host bytes).dedisperse(100): reference block plan "
                           f"({len(blocks)} blocks of {gulp} samples), wall clock"})
+
+
+def run_c3(args, rank, world, local, emit) -> None:
+    """Config 3: 64 beams of uneven length, two-stage subband search (32
+    subbands, 512 trials 0-1000), downsample 1/2/4, boxcar widths 1..256 ->
+    S/N peaks; each batch of beams is one CUDA graph of persistent launches.
+    Also times the plain per-call path (one brute-force dedispersion + S/N per
+    beam and DM) on a subset."""
+    m = measure_c3(steps, warmup, args.beams, args.batch, rank, world)
+    if rank == 0:
+        emit(**m)
+
+
+def measure_c3(steps: int, warmup: int, beams: int, batch: int, rank: int, world: int) -> dict:
+    """Config-3 measurements as the fields of one bench line (see run_c3)."""
+    from .dedisp import dedisperse_block
+    from .search import boxcar_snr
+    from .subband import SubbandPlan, SubbandSearch
+
+    g = synth.C3
+    h = Header(nchans=g.nchans, fch1=g.fch1, foff=g.foff, tsamp=g.tsamp, nbits=8)
+    plan = SubbandPlan(h, synth.dm_grid(500.0, 512), nsub=32, group=16)
+    rng = np.random.default_rng(3)
+    nbeams = beams
+    lens = rng.integers(1 << 18, (1 << 21) + 1, size=nbeams)
+    lo, hi = multi.shard_range(nbeams, rank, world)
+    th = synth.gauss_u8_thresholds(96.0, 12.0)
+    factors, widths = (1, 2, 4), tuple(1 << k for k in range(9))
+    # autotune the two stages on the first batch
+    tune_lens = lens[lo:lo + batch]
+    best, best_ms = (0, 0), None
+    for v1, v2 in ((0, 0), (1, 0), (2, 0), (3, 0)):
+        srch = SubbandSearch(plan, tune_lens, factors=factors, widths=widths, variants=(v1, v2))
+        for b in srch.beams:
+            synth.gauss_u8_device(b.raw.numel(), 99, 96.0, 12.0, out=b.raw)
+        srch.run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        srch.run(snr=False)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if best_ms is None or ms < best_ms:
+            best, best_ms = (v1, v2), ms
+        del srch
+        torch.cuda.empty_cache()
+    v1 = best[0]
+    best_ms = None
+    for v2 in range(4):
+        srch = SubbandSearch(plan, tune_lens, factors=factors, widths=widths, variants=(v1, v2))
+        for b in srch.beams:
+            synth.gauss_u8_device(b.raw.numel(), 99, 96.0, 12.0, out=b.raw)
+        srch.run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        srch.run(snr=False)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        if best_ms is None or ms < best_ms:
+            best, best_ms = (v1, v2), ms
+        del srch
+        torch.cuda.empty_cache()
+    total_ms, units = 0.0, 0
+    peaks = []
+    torch.cuda.synchronize()
+    _barrier(world)
+    for b0 in range(lo, hi, batch):
+        blens = lens[b0:min(hi, b0 + batch)]
+        srch = SubbandSearch(plan, blens, factors=factors, widths=widths, variants=best)
+        for i, b in enumerate(srch.beams):
+            synth.gauss_u8_device(b.raw.numel(), 3000 + b0 + i, 96.0, 12.0, out=b.raw)
+        srch.capture()
+        for _ in range(warmup):
+            srch.replay()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            srch.replay()
+        e1.record()
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1) / steps
+        units += sum(512 * b.nvalid for b in srch.beams)
+        peaks += [float(b.snr.max()) for b in srch.beams]
+        assert srch.status_ok()
+        del srch
+        torch.cuda.empty_cache()
+    ms_max = multi.max_over_ranks(total_ms)
+    units_all = multi.sum_over_ranks(units)
+    value = units_all / (ms_max / 1e3)
+    # plain per-call path on a subset: 2 beams x 16 DMs, brute force + S/N per call
+    nsub_beams, nsub_dms = 2, 16
+    dms = plan.dms[np.linspace(0, 511, nsub_dms).astype(int)]
+    t_plain, u_plain = 0.0, 0
+    for bi in range(nsub_beams):
+        n = int(lens[bi])
+        raw = synth.gauss_u8_device(n * g.nchans, 3000 + bi, 96.0, 12.0)
+        d_all = np.atleast_2d(h.get_dmdelays(dms)).astype(np.int32)
+        tim = torch.empty(n, dtype=torch.float32, device="cuda")
+        for dmi in range(nsub_dms):  # warm
+            dedisperse_block(raw, d_all[dmi], g.nchans, n, tim)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for dmi in range(nsub_dms):
+            d = d_all[dmi]
+            nvi = dedisperse_block(raw, d, g.nchans, n, tim)
+            boxcar_snr(tim[:nvi].view(1, -1), widths=widths, factors=factors)
+            u_plain += nvi
+        torch.cuda.synchronize()
+        t_plain += time.perf_counter() - t0
+    plain = u_plain / t_plain
+    return dict(metric="DM-trial x samples/s, config 3 (batched two-stage subband search + S/N)",
+              value=value, unit=UNIT, n_gpus=world, steps=steps, warmup=warmup,
+              ms_per_step=ms_max, higher_is_better=True, scaling="weak", vs_baseline=None,
+              dtype="u8->uint16->int32 (+f32 S/N)", data="synthetic (device generator, seeded)",
+              config={"workload": f"config 3: {nbeams} beams nsamps U[2^18,2^21], 1024 ch 8-bit, "
+                      "32 subbands x 16-trial groups, 512 trials 0-1000, downsample 1/2/4, "
+                      "widths 1..256", "batch_beams": batch, "variants": list(best),
+                      "beams_total_samples": int(lens.sum())},
+              plain_per_call={"value": plain, "unit": UNIT, "path": "dedisperse_block + boxcar_snr "
+                              "per (beam, DM), brute force over 1024 channels",
+                              "sample": f"{nsub_beams} beams x {nsub_dms} DMs"},
+              served_over_plain=value / plain, max_snr=max(peaks) if peaks else None,
+              gpu_launches=None)
 
 
 def run_c4(args, rank, world, local, emit) -> None:

@@ -27,9 +27,12 @@ def golden_meta():
 
 @pytest.fixture(scope="session")
 def orc():
+    import os
+
     from oracle import oracle
 
     oracle.build()
+    oracle.set_threads(os.cpu_count() or 1)
     return oracle
 
 

@@ -1,9 +1,13 @@
 """Generate golden vectors by running the REFERENCE implementation's own code.
 
-Run in a container where the reference source tree is mounted (path from
-$SPP_REFERENCE_ROOT, default /root/reference):
+Run in a container where the reference source tree is mounted, naming it in
+$SPP_REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py
+    SPP_REFERENCE_ROOT=<path to the reference checkout> python tests/golden/make_golden.py
+
+Besides the vectors it copies the reference's small sigproc test files
+(tests/data/*.fil) into tests/golden/_ref/ (kept out of version control) for
+the real-file tests, which skip when the copies are absent.
 
 It loads src/sigpyproc/core/kernels.py (numba) and single functions of
 params.py / header.py / readers.py through oracle/refload.py, evaluates them
@@ -296,6 +300,56 @@ def main() -> None:
                            "nints": nints, "nbands": nbands, "gulp": gulp, "seed": seed,
                            "input_sha256": sha(data_all)})
     meta["fold_cases"] = fold_cases
+
+    # ---- N1 real files: Filterbank.dedisperse over the reference's sigproc
+    # test files -- its read_plan block loop (readers.py:171-233), its
+    # unpack kernels as FileReader.creadinto applies them (io/fileio.py:284-292,
+    # io/bits.py:175-182 bit orders) and kernels.dedisperse per block
+    # (base.py:400-424)
+    import shutil  # noqa: PLC0415
+
+    from sigpyproc3_b200.io import sigproc as sp  # noqa: PLC0415
+
+    refdir = HERE / "_ref"
+    refdir.mkdir(exist_ok=True)
+    meta["files"] = {}
+    for name, dm in (("parkes_1bit", 100.0), ("parkes_2bit", 100.0), ("parkes_4bit", 100.0),
+                     ("parkes_8bit_1", 100.0), ("parkes_8bit_2", 100.0),
+                     ("tutorial_2bit", 30.0)):
+        src = refload.TEST_DATA / f"{name}.fil"
+        blob = src.read_bytes()
+        hdr = sp.read_header(src)
+        nbits, nch, nsamples = int(hdr["nbits"]), int(hdr["nchans"]), int(hdr["nsamples"])
+        raw = np.frombuffer(blob, dtype=np.uint8)[hdr["hdrlen"]:]
+        order = "little" if nbits == 1 else "big"
+        unpack_fn = getattr(K, f"unpack{nbits}_8_{order}") if nbits < 8 else None
+
+        class FileFake(FakeFile):
+            def creadinto(self, rbuf, ubuf=None):
+                n = super().creadinto(rbuf, ubuf)
+                if unpack_fn is not None:
+                    unpack_fn(np.frombuffer(memoryview(rbuf), dtype=np.uint8),
+                              np.frombuffer(memoryview(ubuf), dtype=np.uint8))
+                return n
+
+        fr = FakeReader(raw, nsamples, nch)
+        fr._file = FileFake(raw)
+        fr.bitsinfo.unpack = nbits < 8
+        fr.samp_stride = nch * nbits // 8
+        fr.chan_stride = nbits / 8
+        d = ref_delays(nch, float(hdr["fch1"]), float(hdr["foff"]), float(hdr["tsamp"]),
+                       dm).astype(np.int32)
+        maxd = int(np.max(np.abs(d)))
+        gulp = max(2 * maxd, 16384)
+        tim = np.zeros(nsamples - maxd, dtype=np.float32)
+        for nsamps_r, ii, data in read_plan(fr, gulp=gulp, skipback=maxd, quiet=True):
+            K.dedisperse(np.ascontiguousarray(data), tim, d, nch, nsamps_r, ii * (gulp - maxd))
+        out[f"file_{name}_tim"] = tim
+        out[f"file_{name}_delays"] = d
+        meta["files"][name] = {"dm": dm, "sha256": hashlib.sha256(blob).hexdigest(),
+                               "nbits": nbits, "nchans": nch, "nsamples": nsamples,
+                               "maxdelay": maxd, "gulp": gulp}
+        shutil.copyfile(src, refdir / f"{name}.fil")
 
     np.savez_compressed(HERE / "golden.npz", **out)
     (HERE / "golden.json").write_text(json.dumps(meta, indent=1))

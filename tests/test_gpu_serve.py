@@ -143,3 +143,55 @@ def test_short_first_chunks(torch_cuda, orc):
         assert max(a.nvalid, 0) == max(c.nvalid, 0)
         if c.nvalid > 0:
             np.testing.assert_array_equal(a.dmt.cpu().numpy(), c.dmt.cpu().numpy())
+
+
+def test_served_wide_beams(torch_cuda, orc):
+    """Config-4-sized beams: 4096 channels of 1- and 2-bit data, chunks of
+    2^14 samples and more, each chunk the same alone, in the mix and in the
+    oracle over the concatenated stream."""
+    torch = torch_cuda
+    from sigpyproc3_b200 import Header
+    from sigpyproc3_b200.serve import BeamSpec, BeamState, Chunk, Server, plain_process
+
+    specs = []
+    for b, (nbits, dmmax, ndm) in enumerate([(2, 500.0, 64), (1, 300.0, 40)]):
+        h = Header(nchans=4096, fch1=1500.0, foff=-300.0 / 4096, tsamp=64e-6, nbits=nbits)
+        specs.append(BeamSpec(b, h, np.linspace(0.0, dmmax, ndm)))
+    rng = np.random.default_rng(44)
+    data = {}
+    for sp in specs:
+        h = sp.header
+        lens = rng.integers(1 << 14, 20000, size=3)
+        vals = [rng.integers(0, 1 << h.nbits, size=n * h.nchans, dtype=np.uint8) for n in lens]
+        order = "little" if h.nbits == 1 else "big"
+        data[sp.beam_id] = (lens, vals, [_pack(v, h.nbits, order) for v in vals])
+    srv = Server(specs, hbm_budget=8 << 30, keep_dmt=True, max_inflight=2)
+    chunks = {}
+    for k in range(3):
+        for sp in specs:
+            lens, _, raws = data[sp.beam_id]
+            c = Chunk(sp.beam_id, k, int(lens[k]), torch.from_numpy(raws[k]).pin_memory())
+            chunks[(sp.beam_id, k)] = c
+            srv.submit(c)
+        srv.step()
+    srv.drain()
+    torch.cuda.synchronize()
+    for sp in specs:
+        b = sp.beam_id
+        lens, vals, raws = data[b]
+        st = BeamState(sp, torch.device("cuda", 0))
+        total = int(lens.sum())
+        ref = orc.dmt(np.concatenate(vals), st.delays, 4096, total, total - st.maxd)
+        pos = 0
+        for k in range(3):
+            mixed = chunks[(b, k)]
+            alone = plain_process(None, Chunk(b, k, int(lens[k]), torch.from_numpy(raws[k])), st,
+                                  keep_dmt=True)
+            assert mixed.nvalid == alone.nvalid
+            if mixed.nvalid <= 0:
+                continue
+            m = mixed.dmt.cpu().numpy()
+            np.testing.assert_array_equal(m, alone.dmt.cpu().numpy())
+            np.testing.assert_array_equal(m, ref[:, pos:pos + mixed.nvalid])
+            pos += mixed.nvalid
+        assert pos == ref.shape[1]

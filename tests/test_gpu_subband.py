@@ -17,10 +17,10 @@ def torch_cuda():
 
 
 def _beam(seed, nsamps, nchans):
-    from sigpyproc3_b200 import synth
+    from oracle import synth_host
 
-    th = synth.gauss_u8_thresholds(96.0, 12.0)
-    return synth.gauss_u8_host(seed, 0, nsamps * nchans, th)
+    th = synth_host.gauss_u8_thresholds(96.0, 12.0)
+    return synth_host.gauss_u8_host(seed, 0, nsamps * nchans, th)
 
 
 def test_subband_search_small(torch_cuda, orc):

@@ -189,3 +189,28 @@ def test_pulse_extractor_window(tmp_path):
         assert (pe.disp_delay, pe.t_decimate, pe.nsamps) == (disp, tdec, n)
         assert pe.nstart == toa - n // 2 and pe.nstart_file == max(0, toa - n // 2)
         assert pe.nsamps_file == min(n + min(0, pe.nstart), 6000 - max(0, pe.nstart))
+
+
+def test_host_twins_follow_the_generator_definitions():
+    """The test suite's numpy twins (oracle/synth_host.py) describe the same
+    config-2 workload as the product's device generator: geometry, trial
+    grid, delay table, pulse rows and threshold tables."""
+    from oracle import synth_host
+    from sigpyproc3_b200 import synth
+
+    g = synth.C2
+    assert (g.nchans, g.nsamps, g.nbits, g.tsamp, g.fch1, g.foff) == (
+        synth_host.C2_NCHANS, synth_host.C2_NSAMPS, synth_host.C2_NBITS, synth_host.C2_TSAMP,
+        synth_host.C2_FCH1, synth_host.C2_FOFF)
+    assert synth.C2_PULSES == synth_host.C2_PULSES
+    assert synth.C2_PULSE_WIDTH == synth_host.C2_PULSE_WIDTH
+    dms = synth.dm_grid(1000.0, 1024)
+    np.testing.assert_array_equal(dms, synth_host.dm_grid(1000.0, 1024))
+    np.testing.assert_array_equal(np.atleast_2d(g.delays(dms)).astype(np.int32),
+                                  synth_host.c2_delays(dms))
+    for a, b in zip(synth.c2_pulse_rows(), synth_host.c2_pulse_rows()):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(synth.gauss_u8_thresholds(96.0, 12.0),
+                                  synth_host.gauss_u8_thresholds(96.0, 12.0))
+    x = synth_host.c2_filterbank_host(199_990, 40)
+    assert x.shape == (40, 1024) and x.dtype == np.uint8

@@ -5,7 +5,10 @@ a real-time pipeline that reserves its memory up front, or a host framework
 whose allocator owns the device memory -- and keeps its scratch in a fixed
 array inside the library.  Checked through the C ABI against the regular
 spp_dedisperse (bit-exact for integer data), on two consecutive calls with
-different inputs, and for its size limit.  Collected last on purpose.
+different inputs, against the oracle's restatement of kernels.dedisperse
+(src/sigpyproc/core/kernels.py:340-362), for its status words (read through
+spp_dedisperse_noalloc_status_read) and for its size limit.  Collected last
+on purpose.
 """
 
 import ctypes
@@ -25,7 +28,13 @@ def _call_regular(lib, torch, x, nbits, nchans, nsamps, d_dev, dmin, dmax, out, 
     assert rc == 0, lib.spp_last_error_string()
 
 
-def test_noalloc_matches_regular_twice():
+def _status(lib, st):
+    words = np.zeros(4, dtype=np.uint32)
+    rc = lib.spp_dedisperse_noalloc_status_read(words.ctypes.data, st)
+    return rc, words
+
+
+def test_noalloc_matches_regular_twice(orc):
     import torch
 
     from sigpyproc3_b200 import _lib
@@ -46,6 +55,8 @@ def test_noalloc_matches_regular_twice():
             for k in range(4):
                 packed |= (vals[k::4] << (6 - 2 * k)).astype(np.uint8)
             vals = packed
+        expect = orc.dedisperse(vals if nbits == 8 else orc.unpack(vals, 2, "big"), d, 256,
+                                nsamps)
         x = torch.from_numpy(vals).cuda()
         d_dev = torch.from_numpy(d).cuda()
         nv = nsamps - max(abs(dmin), abs(dmax))
@@ -61,6 +72,43 @@ def test_noalloc_matches_regular_twice():
         if call > 0:  # the first call looks up the scratch address; none allocates
             assert torch.cuda.mem_get_info()[0] == free0
         np.testing.assert_array_equal(out.cpu().numpy(), ref.cpu().numpy())
+        np.testing.assert_array_equal(out.cpu().numpy(), expect)
+        rc, words = _status(lib, st)
+        assert rc == _lib.SPP_OK and words[0] == 0, words
+
+
+def test_noalloc_status_reports_clamped_delays(orc):
+    """A declared delay range narrower than the table: the kernel clamps the
+    outliers (no access leaves the staged rows), flags them, and the status
+    read reports it; the next correct call clears the flag."""
+    import torch
+
+    from sigpyproc3_b200 import _lib
+    from sigpyproc3_b200.header import Header
+
+    lib = _lib.load()
+    st = torch.cuda.current_stream().cuda_stream
+    h = Header(nchans=256, fch1=1500.0, foff=-1.0, tsamp=64e-6, nbits=8)
+    nsamps = 16384
+    d = np.atleast_1d(h.get_dmdelays(100.0)).astype(np.int32)
+    vals = np.random.default_rng(7).integers(0, 256, size=nsamps * 256, dtype=np.uint8)
+    x = torch.from_numpy(vals).cuda()
+    d_dev = torch.from_numpy(d).cuda()
+    dmin, dmax = int(d.min()), int(d.max())
+    out = torch.zeros(nsamps, device="cuda")
+    rc = lib.spp_dedisperse_noalloc(x.data_ptr(), 8, 0, 256, nsamps, d_dev.data_ptr(), dmin,
+                                    dmax - 300, out.data_ptr(), out.numel(), 0, _lib.ACC_F64, st)
+    assert rc == _lib.SPP_OK
+    rc, words = _status(lib, st)
+    assert rc == _lib.SPP_ERR_DEVICE and (words[0] & 2), words
+    assert b"device status" in ctypes.string_at(lib.spp_last_error_string())
+    rc = lib.spp_dedisperse_noalloc(x.data_ptr(), 8, 0, 256, nsamps, d_dev.data_ptr(), dmin, dmax,
+                                    out.data_ptr(), out.numel(), 0, _lib.ACC_F64, st)
+    assert rc == _lib.SPP_OK
+    rc, words = _status(lib, st)
+    assert rc == _lib.SPP_OK and words[0] == 0, words
+    np.testing.assert_array_equal(out[:nsamps - dmax].cpu().numpy(),
+                                  orc.dedisperse(vals, d, 256, nsamps))
 
 
 def test_noalloc_rejects_oversized_block():
