@@ -229,6 +229,31 @@ def e2e_parity(nchans: int, nbits: int, nsamps: int, delays: np.ndarray, host_in
             "seconds": round(time.perf_counter() - t0, 1)}
 
 
+def c5_accuracy(x, bp, out, d: np.ndarray, nchans: int, nsamps: int, nrows: int = 8,
+                window: int = 8192) -> dict:
+    """Per-result error of the DM-time output against float64 sums: `nrows`
+    trials spread over the grid, the first `window` outputs, recomputed by the
+    oracle from the same input (zero-DM with the run's bandpass, which equals
+    the oracle's sequential float32 bandpass bit for bit)."""
+    from oracle import oracle as orc
+
+    orc.build()
+    orc.set_threads(os.cpu_count() or 1)
+    rows = np.unique(np.linspace(0, d.shape[0] - 1, nrows).astype(int))
+    nin = window + int(d[rows].max())
+    xh = x[: nin * nchans].cpu().numpy()
+    bph = bp.cpu().numpy()
+    y = orc.zero_dm(xh, nchans, nin, bph)
+    ref32, ref64 = orc.dmt(y, d[rows], nchans, nin, window, want64=True)
+    got = out[rows, :window].cpu().numpy()
+    err = np.abs(got.astype(np.float64) - ref64)
+    rel = err / np.maximum(np.abs(ref64), np.finfo(np.float64).tiny)
+    return {"rows": [int(r) for r in rows], "samples_per_row": window,
+            "max_rel_err": float(rel.max()), "frac_beyond_rtol_1e-5": float(np.mean(rel > 1e-5)),
+            "bit_identical_to_oracle": bool(np.array_equal(got, ref32)),
+            "checked_against": "oracle float64 channel-ordered sums"}
+
+
 def run_gpu(args, rank, world, local):
     import torch
 
@@ -396,6 +421,8 @@ def main():
                     help="output samples per host-streaming block in the e2e leg")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the e2e row check")
+    ap.add_argument("--acc", choices=["f64", "kahan"], default="f64",
+                    help="config 5: float accumulator")
     ap.add_argument("--no-secondary", action="store_true", help="skip the config 1/3 blocks")
     ap.add_argument("--variant", type=int, default=None, help="fix the kernel variant")
     ap.add_argument("--workload", choices=["c2", "c3", "c4", "c1", "c5", "snr", "fold"], default="c2")
@@ -418,7 +445,8 @@ def main():
         else:
             from sigpyproc3_b200 import workloads
 
-            workloads.run(args.workload, args, rank, world, local, _line)
+            checks = {} if args.no_parity else {"c5": c5_accuracy}
+            workloads.run(args.workload, args, rank, world, local, _line, checks)
     finally:
         if world > 1:
             import torch.distributed as dist

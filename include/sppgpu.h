@@ -262,6 +262,31 @@ int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n,
                    const int32_t* widths, int nwidths, float* snr,
                    int32_t* peak_index, void* workspace,
                    int64_t workspace_bytes, void* stream);
+/* TimeSeries.apply_boxcar (timeseries.py:296-325) with stats.running_filter
+ * "mean" (core/stats.py:200-243): out[(i + ref_bin) mod n] = f32(sqrt(w) *
+ * mean(p[i .. i+w-1])), p = the n samples padded symmetrically (np.pad
+ * "symmetric") by w/2 on the left and w/2 (odd w) or w/2-1 (even w) on the
+ * right, ref_bin = -w/2 + 1 (odd w) or -w/2 (even w).  Window sums in float64
+ * (the reference's bottleneck.move_mean keeps a float32 running sum).
+ * 1 <= width <= 8192; `in` and `out` distinct device arrays of n floats. */
+int spp_boxcar_filter(const float* in, int64_t n, int width, float* out,
+                      void* stream);
+
+/* The same with the robust location and scale of the reference MatchedFilter's
+ * defaults (core/filters.py:105-125: stats.estimate_zscore with loc_method
+ * "median", scale_method "iqr", core/stats.py:418-502): per row and factor,
+ *   loc   = median of y (float32; the two middle values averaged in float32)
+ *   scale = (q75 - q25) / 1.3489795003921634 (float64; numpy's linear
+ *           percentile interpolation; 1 when ~0)
+ *   snr   = max_t (sum_{k<w} y[t+k] - w*loc) / (scale * sqrt(w)).
+ * The order statistics are exact (radix selection over the float32 y). */
+int64_t spp_boxcar_snr_robust_workspace_bytes(int64_t nrows, int64_t n,
+                                              int nfactors, int nwidths);
+int spp_boxcar_snr_robust(const void* in, int in_kind, int64_t nrows,
+                          int64_t n, int64_t in_stride, const int32_t* factors,
+                          int nfactors, const int32_t* widths, int nwidths,
+                          float* snr, int32_t* peak_index, void* workspace,
+                          int64_t workspace_bytes, void* stream);
 
 /* ---- R7: subband dedispersion ----------------------------------------------------
  * Stage 1 replaces kernels.subband (core/kernels.py:379-401) with a zeroed

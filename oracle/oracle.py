@@ -10,6 +10,7 @@ fixtures in ``tests/golden/``.
 from __future__ import annotations
 
 import ctypes
+import math
 import subprocess
 from pathlib import Path
 
@@ -57,6 +58,9 @@ def lib() -> ctypes.CDLL:
             "orc_zero_dm_f32": ([_p, _p, _i64, _i64, _p, _p], None),
             "orc_downsample_mean": ([_p, _i64, ctypes.c_int, _p], None),
             "orc_boxcar_snr_row": ([_p, _i64, _p, ctypes.c_int, _p, ctypes.c_int, _p, _p], None),
+            "orc_boxcar_snr_row_ls": ([_p, _i64, _p, ctypes.c_int, _p, ctypes.c_int, ctypes.c_int,
+                                       _p, _p, _p, _p], None),
+            "orc_median_iqr": ([_p, _i64, _p, _p], None),
             "orc_subband_u8": ([_p, _p, _p, _p, _i64, _i64, _i64, _i64], None),
             "orc_py_floordiv": ([ctypes.c_double, ctypes.c_double], ctypes.c_double),
             "orc_fold_block": ([_p, ctypes.c_int, _p, _p, _p, _i32, ctypes.c_float,
@@ -213,18 +217,52 @@ def downsample_mean(x: np.ndarray, factor: int) -> np.ndarray:
     return out
 
 
-def boxcar_snr(rows: np.ndarray, factors, widths):
-    """Boxcar S/N peaks per row (float64) and argmax indices."""
+def boxcar_snr(rows: np.ndarray, factors, widths, loc_scale: str = "mean_std",
+               return_loc_scale: bool = False):
+    """Boxcar S/N peaks per row (float64) and argmax indices: TimeSeries.downsample
+    (timeseries.py:107-132) then a square-normalised boxcar (apply_boxcar,
+    timeseries.py:296-325) over the series z-scored by stats.estimate_zscore
+    (core/stats.py:418-502) with loc/scale "mean_std" or "median_iqr"."""
     rows = np.atleast_2d(rows)
     factors = np.ascontiguousarray(factors, dtype=np.int32)
     widths = np.ascontiguousarray(widths, dtype=np.int32)
     snr = np.zeros((rows.shape[0], factors.size, widths.size), dtype=np.float64)
     idx = np.zeros(snr.shape, dtype=np.int32)
+    locs = np.zeros((rows.shape[0], factors.size), dtype=np.float64)
+    scales = np.zeros_like(locs)
+    robust = {"mean_std": 0, "median_iqr": 1}[loc_scale]
     for r in range(rows.shape[0]):
         row = np.ascontiguousarray(rows[r], dtype=np.float32)
-        lib().orc_boxcar_snr_row(_ptr(row), row.size, _ptr(factors), factors.size, _ptr(widths),
-                                 widths.size, snr[r].ctypes.data, idx[r].ctypes.data)
+        lib().orc_boxcar_snr_row_ls(_ptr(row), row.size, _ptr(factors), factors.size,
+                                    _ptr(widths), widths.size, robust, snr[r].ctypes.data,
+                                    idx[r].ctypes.data, locs[r].ctypes.data,
+                                    scales[r].ctypes.data)
+    if return_loc_scale:
+        return snr, idx, locs, scales
     return snr, idx
+
+
+def apply_boxcar(x: np.ndarray, width: int) -> np.ndarray:
+    """TimeSeries.apply_boxcar (timeseries.py:296-325) over stats.running_filter
+    "mean" (core/stats.py:200-243): np.pad "symmetric", window means (exact
+    float64 window sums here; the reference's bottleneck keeps a float32
+    running sum), times sqrt(width), np.roll by the reference bin."""
+    x = np.asarray(x, dtype=np.float32)
+    pad = (width // 2, width // 2) if width % 2 else (width // 2, width // 2 - 1)
+    xp = np.pad(x, pad, "symmetric").astype(np.float64)
+    win = np.lib.stride_tricks.sliding_window_view(xp, width)
+    mean = np.fromiter((math.fsum(w_) for w_ in win), dtype=np.float64, count=win.shape[0]) / width
+    out = (mean * math.sqrt(width)).astype(np.float32)
+    ref_bin = -width // 2 + 1 if width % 2 else -width // 2
+    return np.roll(out, ref_bin)
+
+
+def median_iqr(y: np.ndarray) -> tuple[float, float]:
+    """(median, IQR / 1.349) of float32 values as stats.estimate_zscore computes them."""
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    loc, scale = ctypes.c_double(), ctypes.c_double()
+    lib().orc_median_iqr(_ptr(y), y.size, ctypes.byref(loc), ctypes.byref(scale))
+    return loc.value, scale.value
 
 
 def subband(data: np.ndarray, delays: np.ndarray, chan_to_sub: np.ndarray, maxdelay: int,

@@ -135,3 +135,13 @@ def load_read_plan():
     }
     exec(compile("from __future__ import annotations\n" + src, "readers.py", "exec"), ns)
     return ns["read_plan"]
+
+
+def load_scale_iqr():
+    """Reference ``stats._scale_iqr`` (core/stats.py:480-502), executed as-is."""
+    import numpy as np
+
+    src = _extract(SRC / "core" / "stats.py", {"_scale_iqr"})
+    ns: dict = {"np": np, "NDArray": object}
+    exec(compile("from __future__ import annotations\n" + src, "stats.py", "exec"), ns)
+    return ns["_scale_iqr"]

@@ -246,8 +246,63 @@ void orc_downsample_mean(const float* in, int64_t n, int factor, float* out) {
  *   y = downsample_1d_mean(x, f) (values rounded to float32 as the reference)
  *   snr_w = max_t (sum_{k<w} y[t+k] - w*mean(y)) / (std(y) * sqrt(w)).
  * Writes snr[fi*nwidths + wi] and the argmax t to idx (may be NULL). */
+static int cmp_f32(const void* a, const void* b) {
+  const float x = *(const float*)a, y = *(const float*)b;
+  return (x > y) - (x < y);
+}
+
+/* numpy's linear-interpolation quantile of sorted float32 values, in float64
+ * (numpy _quantile / _lerp: index (n-1)*q, lerp from the far end when the
+ * fraction is >= 0.5). */
+static double quantile_linear(const float* v, int64_t m, double q) {
+  const double vi = (double)(m - 1) * q;
+  int64_t lo = (int64_t)floor(vi);
+  int64_t hi = lo + 1;
+  if (vi >= (double)(m - 1)) lo = hi = m - 1;
+  const double g = vi - (double)lo;
+  const double a = (double)v[lo], b = (double)v[hi];
+  const double diff = b - a;
+  return g >= 0.5 ? b - diff * (1.0 - g) : a + diff * g;
+}
+
+/* stats.estimate_zscore(loc_method="median", scale_method="iqr")
+ * (core/stats.py:418-502) location and scale of float32 values:
+ * loc = np.median (float32: mean of the two middle values for an even count),
+ * scale = (q75 - q25) / 1.3489795003921634 in float64, replaced by 1 when it
+ * is ~0 (np.isclose(scale, 0)). */
+void orc_median_iqr(const float* y, int64_t m, double* loc, double* scale) {
+  float* v = (float*)malloc(sizeof(float) * (m > 0 ? m : 1));
+  memcpy(v, y, sizeof(float) * m);
+  qsort(v, (size_t)m, sizeof(float), cmp_f32);
+  float med;
+  if (m & 1) {
+    med = v[(m - 1) / 2];
+  } else {
+    volatile float sum = v[m / 2 - 1] + v[m / 2];
+    med = sum / 2.0f;
+  }
+  *loc = (double)med;
+  double sc = (quantile_linear(v, m, 0.75) - quantile_linear(v, m, 0.25)) / 1.3489795003921634;
+  if (fabs(sc) <= 1e-8) sc = 1.0;
+  *scale = sc;
+  free(v);
+}
+
+void orc_boxcar_snr_row_ls(const float* x, int64_t n, const int32_t* factors, int nfactors,
+                           const int32_t* widths, int nwidths, int robust, double* snr,
+                           int32_t* idx, double* locs, double* scales);
+
 void orc_boxcar_snr_row(const float* x, int64_t n, const int32_t* factors, int nfactors,
                         const int32_t* widths, int nwidths, double* snr, int32_t* idx) {
+  orc_boxcar_snr_row_ls(x, n, factors, nfactors, widths, nwidths, 0, snr, idx, NULL, NULL);
+}
+
+/* Boxcar S/N of one row per downsample factor and width, with location and
+ * scale either mean / population std (robust = 0) or median / IQR (robust =
+ * 1):  snr = max_t (sum_{k<w} y[t+k] - w * loc) / (scale * sqrt(w)). */
+void orc_boxcar_snr_row_ls(const float* x, int64_t n, const int32_t* factors, int nfactors,
+                           const int32_t* widths, int nwidths, int robust, double* snr,
+                           int32_t* idx, double* locs, double* scales) {
   float* y = (float*)malloc(sizeof(float) * (n > 0 ? n : 1));
   double* pre = (double*)malloc(sizeof(double) * (n + 1));
   for (int fi = 0; fi < nfactors; ++fi) {
@@ -267,6 +322,10 @@ void orc_boxcar_snr_row(const float* x, int64_t n, const int32_t* factors, int n
     }
     double sd = m > 0 ? sqrt(ss / (double)m) : 0.0;
     if (sd == 0.0) sd = 1.0;
+    double loc = mean;
+    if (robust && m > 0) orc_median_iqr(y, m, &loc, &sd);
+    if (locs) locs[fi] = loc;
+    if (scales) scales[fi] = sd;
     for (int wi = 0; wi < nwidths; ++wi) {
       const int w = widths[wi];
       double best = -INFINITY;
@@ -275,7 +334,7 @@ void orc_boxcar_snr_row(const float* x, int64_t n, const int32_t* factors, int n
         const double v = pre[t + w] - pre[t];
         if (v > best) { best = v; bt = t; }
       }
-      snr[fi * nwidths + wi] = bt < 0 ? NAN : (best - (double)w * mean) / (sd * sqrt((double)w));
+      snr[fi * nwidths + wi] = bt < 0 ? NAN : (best - (double)w * loc) / (sd * sqrt((double)w));
       if (idx) idx[fi * nwidths + wi] = (int32_t)bt;
     }
   }

@@ -77,6 +77,10 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_boxcar_snr_workspace_bytes": ([_i64, _i64, _int, _int], _i64),
     "spp_boxcar_snr": ([_p, _int, _i64, _i64, _i64, _p, _int, _p, _int, _p, _p, _p, _i64, _p],
                        _int),
+    "spp_boxcar_filter": ([_p, _i64, _int, _p, _p], _int),
+    "spp_boxcar_snr_robust_workspace_bytes": ([_i64, _i64, _int, _int], _i64),
+    "spp_boxcar_snr_robust": ([_p, _int, _i64, _i64, _i64, _p, _int, _p, _int, _p, _p, _p, _i64,
+                               _p], _int),
     "spp_subband": ([_p, _int, _int, _i64, _i64, _p, _i32, _p, _i64, _p, _p], _int),
     "spp_wl_num_variants": ([_int, _int], _int),
     "spp_wl_describe": ([_int, _int, _int, _p], _int),

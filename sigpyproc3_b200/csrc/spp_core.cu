@@ -133,7 +133,10 @@ static const std::vector<Variant>& variants() {
       mk<32, 16, 4, 1, 16, 2, SPP_ACC_KAHAN32>(0),
       mk<32, 8, 2, 1, 16, 2, SPP_ACC_KAHAN32>(0),
       mk<32, 16, 2, 1, 16, 2, SPP_ACC_KAHAN32>(0),
-      // float32 input, fp64 accumulator
+      // float32 input, fp64 accumulator (channel-ordered sums: the reference's)
+      mk<32, 16, 4, 1, 16, 2, SPP_ACC_F64>(0),
+      mk<32, 16, 2, 1, 16, 2, SPP_ACC_F64>(0),
+      mk<32, 8, 2, 1, 16, 2, SPP_ACC_F64>(0),
       mk<32, 8, 8, 1, 32, 2, SPP_ACC_F64>(0),
       mk<32, 4, 8, 2, 32, 2, SPP_ACC_F64>(0),
       mk<32, 8, 4, 1, 16, 2, SPP_ACC_F64>(0),
@@ -739,8 +742,8 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
   }
   int rc = SPP_OK;
   if (zd_rows) {
-    const unsigned blocks = (unsigned)ceil_div(nsamps, 8);
-    k_row_sum_f64<<<blocks, 256, 0, st>>>(static_cast<const float*>(in), p->nchans, nsamps, zd_rows);
+    const unsigned blocks = (unsigned)ceil_div(nsamps, 32 * kRowSumWarps);
+    k_row_sum_f64<<<blocks, 32 * kRowSumWarps, 0, st>>>(static_cast<const float*>(in), p->nchans, nsamps, zd_rows);
     rc = cuda_status(cudaGetLastError(), "zero-DM row sums");
     if (rc) return rc;
   }

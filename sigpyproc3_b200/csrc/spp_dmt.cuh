@@ -173,16 +173,31 @@ k_corner_turn_f32(const float* __restrict__ raw, int64_t nchans, int64_t nsamps,
 }
 
 // Per-sample zero-DM sums zdm[t] = sum_c f64(x[t][c]) (one warp per sample).
-static __global__ void k_row_sum_f64(const float* __restrict__ raw, int64_t nchans, int64_t nsamps,
-                              double* __restrict__ zdm) {
-  const int64_t t = (int64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (t >= nsamps) return;
+// zdm[t] = sum_c f64(x[t][c]), added in channel order (the order of the
+// kernels.remove_zerodm loop, core/kernels.py:497-499): a warp owns 32 rows,
+// stages 32 x 32 tiles through shared memory with coalesced loads, and each
+// lane adds its row's channels one by one.
+constexpr int kRowSumWarps = 8;
+static __global__ void __launch_bounds__(kRowSumWarps * 32)
+k_row_sum_f64(const float* __restrict__ raw, int64_t nchans, int64_t nsamps,
+              double* __restrict__ zdm) {
+  __shared__ float tile[kRowSumWarps][32][33];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t t0 = ((int64_t)blockIdx.x * kRowSumWarps + warp) * 32;
+  if (t0 >= nsamps) return;
   double s = 0.0;
-  for (int64_t c = lane; c < nchans; c += 32) s += (double)__ldg(raw + t * nchans + c);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) zdm[t] = s;
+  for (int64_t c0 = 0; c0 < nchans; c0 += 32) {
+    const int64_t c = c0 + lane;
+    for (int r = 0; r < 32; ++r) {
+      const int64_t t = t0 + r;
+      tile[warp][r][lane] = (t < nsamps && c < nchans) ? __ldg(raw + t * nchans + c) : 0.f;
+    }
+    __syncwarp();
+    const int nc = (nchans - c0) < 32 ? (int)(nchans - c0) : 32;
+    for (int j = 0; j < nc; ++j) s = __dadd_rn(s, (double)tile[warp][lane][j]);
+    __syncwarp();
+  }
+  if (t0 + lane < nsamps) zdm[t0 + lane] = s;
 }
 
 // ----------------------------------------------------------------------------

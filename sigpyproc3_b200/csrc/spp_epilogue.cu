@@ -60,32 +60,86 @@ __global__ void k_collapse(const void* __restrict__ in, int64_t nchans, int64_t 
   if (lane == 0) tim[out_start + t] = (float)s;
 }
 
-// zero-DM on time-major float32 (kernels.remove_zerodm): one block per sample.
-__global__ void k_zero_dm(const float* __restrict__ in, float* __restrict__ out, int64_t nchans,
-                          int64_t nsamps, const float* __restrict__ bpass,
-                          const float* __restrict__ chanwts) {
-  __shared__ double red[32];
-  for (int64_t t = blockIdx.x; t < nsamps; t += gridDim.x) {
+// zero-DM on time-major float32 (kernels.remove_zerodm, core/kernels.py:493-505):
+// a block of 8 warps takes 256 samples; each warp sums 32 samples' channels in
+// channel order (32 x 32 tiles staged through shared memory, one lane per
+// sample), then the block rewrites the 256 spectra with coalesced accesses.
+constexpr int kZdmRows = 256;
+__global__ void __launch_bounds__(kZdmRows)
+k_zero_dm(const float* __restrict__ in, float* __restrict__ out, int64_t nchans, int64_t nsamps,
+          const float* __restrict__ bpass, const float* __restrict__ chanwts) {
+  __shared__ float tile[kZdmRows / 32][32][33];
+  __shared__ double zs[kZdmRows];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int64_t tb = (int64_t)blockIdx.x * kZdmRows; tb < nsamps; tb += (int64_t)gridDim.x * kZdmRows) {
+    const int64_t t0 = tb + warp * 32;
     double s = 0.0;
-    for (int64_t c = threadIdx.x; c < nchans; c += blockDim.x) s += (double)in[t * nchans + c];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    for (int64_t c0 = 0; c0 < nchans; c0 += 32) {
+      const int64_t c = c0 + lane;
+      for (int r = 0; r < 32; ++r) {
+        const int64_t t = t0 + r;
+        tile[warp][r][lane] = (t < nsamps && c < nchans) ? __ldg(in + t * nchans + c) : 0.f;
+      }
+      __syncwarp();
+      const int nc = (nchans - c0) < 32 ? (int)(nchans - c0) : 32;
+      for (int j = 0; j < nc; ++j) s = __dadd_rn(s, (double)tile[warp][lane][j]);
+      __syncwarp();
+    }
+    zs[threadIdx.x] = s;
     __syncthreads();
-    if (threadIdx.x < 32) {
-      double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if (threadIdx.x == 0) red[0] = v;
+    const int64_t rows = imin64(kZdmRows, nsamps - tb);
+    for (int64_t r = 0; r < rows; ++r) {
+      const double z = zs[r];
+      const float* src = in + (tb + r) * nchans;
+      float* dst = out + (tb + r) * nchans;
+      for (int64_t c = threadIdx.x; c < nchans; c += kZdmRows) {
+        const double t1 = __dmul_rn(z, (double)chanwts[c]);
+        const double t2 = __dsub_rn((double)src[c], t1);
+        dst[c] = (float)__dadd_rn(t2, (double)bpass[c]);
+      }
     }
     __syncthreads();
-    const double z = red[0];
-    for (int64_t c = threadIdx.x; c < nchans; c += blockDim.x) {
-      const double t1 = __dmul_rn(z, (double)chanwts[c]);
-      const double t2 = __dsub_rn((double)in[t * nchans + c], t1);
-      out[t * nchans + c] = (float)__dadd_rn(t2, (double)bpass[c]);
-    }
-    __syncthreads();
+  }
+}
+
+// TimeSeries.apply_boxcar (timeseries.py:296-325) over stats.running_filter
+// "mean" (core/stats.py:200-243): the series padded symmetrically (np.pad
+// "symmetric", a reflection of period 2n), the mean of each window of
+// `width` samples times sqrt(width), rolled by ref_bin.  A CTA computes
+// kBoxT consecutive window positions i (pre-roll): it stages the padded samples
+// they cover in shared memory, each thread sums its first window in float64
+// and slides it across kBoxR positions, and writes out[(i + ref_bin) mod n].
+constexpr int kBoxThreads = 256;
+constexpr int kBoxR = 16;
+constexpr int kBoxT = kBoxThreads * kBoxR;
+
+__device__ __forceinline__ int64_t sym_index(int64_t k, int64_t n) {
+  int64_t m = k % (2 * n);
+  if (m < 0) m += 2 * n;
+  return m < n ? m : 2 * n - 1 - m;
+}
+
+__global__ void __launch_bounds__(kBoxThreads)
+k_boxcar_filter(const float* __restrict__ in, int64_t n, int width, int64_t pad_left,
+                int64_t ref_bin, float* __restrict__ out) {
+  extern __shared__ float sx[];  // kBoxT + width - 1
+  const int64_t i0 = (int64_t)blockIdx.x * kBoxT;
+  const int64_t len = imin64(kBoxT, n - i0) + width - 1;
+  for (int64_t k = threadIdx.x; k < len; k += kBoxThreads)
+    sx[k] = __ldg(in + sym_index(i0 - pad_left + k, n));
+  __syncthreads();
+  const int64_t a = (int64_t)threadIdx.x * kBoxR;  // this thread's first position
+  if (i0 + a >= n) return;
+  const int cnt = (int)imin64(kBoxR, n - i0 - a);
+  const double norm = sqrt((double)width);
+  double s = 0.0;
+  for (int k = 0; k < width; ++k) s += (double)sx[a + k];
+  for (int r = 0; r < cnt; ++r) {
+    if (r > 0) s = (s + (double)sx[a + r + width - 1]) - (double)sx[a + r - 1];
+    const int64_t i = i0 + a + r;
+    int64_t j = (i + ref_bin) % n;
+    if (j < 0) j += n;
+    out[j] = (float)(s / (double)width * norm);
   }
 }
 
@@ -334,7 +388,7 @@ k_snr_chunk(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
 
 __global__ void k_snr_final(int64_t n, const SnrCfg cfg, int64_t nrows, int64_t nchunks, const SnrPart* __restrict__ parts,
                             const double* __restrict__ stats, float* __restrict__ snr,
-                            int32_t* __restrict__ peak) {
+                            int32_t* __restrict__ peak, const double* __restrict__ locscale) {
   const int nfactors = cfg.nf, nwidths = cfg.nw;
   const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= nrows * nfactors * nwidths) return;
@@ -358,6 +412,10 @@ __global__ void k_snr_final(int64_t n, const SnrCfg cfg, int64_t nrows, int64_t 
   }
   double sd = cnt > 0 ? sqrt(m2 / cnt) : 0.0;
   if (sd == 0.0) sd = 1.0;
+  if (locscale) {  // median / IQR scale computed by k_row_quantiles
+    mean = locscale[rf * 2];
+    sd = locscale[rf * 2 + 1];
+  }
   double best = -DBL_MAX;
   long long bidx = -1;
   for (int64_t k = 0; k < nck; ++k) {
@@ -368,6 +426,149 @@ __global__ void k_snr_final(int64_t n, const SnrCfg cfg, int64_t nrows, int64_t 
   const int w = cfg.w[wi];
   snr[id] = bidx < 0 ? NAN : (float)((best - (double)w * mean) / (sd * sqrt((double)w)));
   if (peak) peak[id] = (int32_t)bidx;
+}
+
+// ---------------------------------------------------------------------------
+// Median / IQR of each downsampled row (the S/N epilogue's robust z-score:
+// stats.estimate_zscore with loc "median" and scale "iqr", core/stats.py:
+// 418-502).  One CTA per (row, factor): the y values (the same float32
+// downsampled means as k_snr_chunk) are mapped to order-preserving 32-bit keys
+// and the needed order statistics are found exactly by radix selection, three
+// passes of 11/11/10-bit digits with one shared-memory histogram per distinct
+// key prefix (warp-aggregated increments).  Up to six ranks: the two middle
+// values (median) and the two neighbours of each quartile's index (q25, q75,
+// linear interpolation as numpy's percentile).
+// ---------------------------------------------------------------------------
+constexpr int kQThreads = 256;
+constexpr int kQBits = 11;
+constexpr int kQBins = 1 << kQBits;
+constexpr int kQRanks = 6;
+
+__device__ __forceinline__ uint32_t f32_key(float v) {
+  const uint32_t b = __float_as_uint(v);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+__device__ __forceinline__ float key_f32(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+__device__ __forceinline__ float snr_y(const char* base, int kind, int64_t i, int f, bool pow2,
+                                       double inv) {
+  double s = 0.0;
+  const int64_t x0 = i * f;
+  for (int q = 0; q < f; ++q) s += row_val(base, kind, x0 + q);
+  return (float)(pow2 ? s * inv : s / f);
+}
+
+__device__ __forceinline__ double quantile_lerp(double a, double b, double g) {
+  const double diff = b - a;  // numpy _lerp: from the far end when g >= 0.5
+  return g >= 0.5 ? b - diff * (1.0 - g) : a + diff * g;
+}
+
+__global__ void __launch_bounds__(kQThreads)
+k_row_quantiles(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
+                const SnrCfg cfg, double* __restrict__ locscale) {
+  extern __shared__ uint32_t qhist[];  // kQRanks x kQBins
+  __shared__ uint32_t pre[kQRanks];    // key prefix per rank (bits above the digit)
+  __shared__ int64_t rnk[kQRanks];     // rank within the prefix
+  __shared__ uint32_t dpre[kQRanks];   // distinct prefixes this pass
+  __shared__ int slot[kQRanks];        // rank -> distinct-prefix histogram
+  __shared__ int ndist;
+  const int64_t row = blockIdx.x / cfg.nf;
+  const int fi = blockIdx.x % cfg.nf;
+  const int f = cfg.f[fi];
+  const int64_t m = n / f;
+  const char* base = static_cast<const char*>(in) + row * in_stride * 4;
+  const bool pow2 = (f & (f - 1)) == 0;
+  const double inv = 1.0 / (double)f;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // ranks: median pair, then q25 and q75 neighbours (0-based, in [0, m))
+  const double v25 = (double)(m - 1) * 0.25, v75 = (double)(m - 1) * 0.75;
+  const int64_t l25 = (int64_t)floor(v25), l75 = (int64_t)floor(v75);
+  if (threadIdx.x == 0) {
+    const int64_t r[kQRanks] = {(m - 1) / 2, m / 2, l25, l25 + 1 < m ? l25 + 1 : m - 1,
+                                l75, l75 + 1 < m ? l75 + 1 : m - 1};
+    for (int t = 0; t < kQRanks; ++t) { pre[t] = 0u; rnk[t] = r[t]; }
+  }
+  __syncthreads();
+  const int shifts[3] = {21, 10, 0};
+  const int widths[3] = {11, 11, 10};
+  for (int pass = 0; pass < 3; ++pass) {
+    const int sh = shifts[pass], wb = widths[pass];
+    const uint32_t hi_mask = (sh + wb >= 32) ? 0u : ~((1u << (sh + wb)) - 1u);
+    const uint32_t dmask = (1u << wb) - 1u;
+    if (threadIdx.x == 0) {
+      int nd = 0;
+      for (int t = 0; t < kQRanks; ++t) {
+        int k = 0;
+        while (k < nd && dpre[k] != pre[t]) ++k;
+        if (k == nd) dpre[nd++] = pre[t];
+        slot[t] = k;
+      }
+      ndist = nd;
+    }
+    for (int i = threadIdx.x; i < kQRanks * kQBins; i += kQThreads) qhist[i] = 0u;
+    __syncthreads();
+    const int nd = ndist;
+    const int64_t mr = (m + kQThreads - 1) / kQThreads * kQThreads;  // whole warps iterate
+    for (int64_t i = threadIdx.x; i < mr; i += kQThreads) {
+      int id = -1;
+      if (i < m) {
+        const uint32_t key = f32_key(snr_y(base, kind, i, f, pow2, inv));
+        const uint32_t hp = key & hi_mask;
+        for (int k = 0; k < nd; ++k)
+          if (dpre[k] == hp) { id = k * kQBins + (int)((key >> sh) & dmask); break; }
+      }
+      const unsigned peers = __match_any_sync(0xffffffffu, id);
+      if (id >= 0 && lane == __ffs(peers) - 1) atomicAdd(&qhist[id], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    // one warp per rank: the digit whose cumulative count passes the rank
+    if (warp < kQRanks) {
+      const uint32_t* h = qhist + slot[warp] * kQBins;
+      constexpr int per = kQBins / 32;
+      uint32_t sum = 0;
+      for (int j = 0; j < per; ++j) sum += h[lane * per + j];
+      uint32_t incl = sum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int64_t r = rnk[warp];
+      const uint32_t excl = incl - sum;
+      const unsigned hit = __ballot_sync(0xffffffffu, (int64_t)excl <= r && r < (int64_t)incl);
+      const int src = __ffs(hit) - 1;
+      if (lane == src) {
+        int64_t c = excl;
+        int d = lane * per;
+        for (int j = 0; j < per; ++j, ++d) {
+          if (r < c + (int64_t)h[d]) break;
+          c += h[d];
+        }
+        rnk[warp] = r - c;
+        pre[warp] |= (uint32_t)d << sh;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    float med;
+    if (m & 1) {
+      med = key_f32(pre[0]);
+    } else {
+      med = __fmul_rn(__fadd_rn(key_f32(pre[0]), key_f32(pre[1])), 0.5f);
+    }
+    const double q25 = quantile_lerp((double)key_f32(pre[2]), (double)key_f32(pre[3]),
+                                     v25 - (double)l25);
+    const double q75 = quantile_lerp((double)key_f32(pre[4]), (double)key_f32(pre[5]),
+                                     v75 - (double)l75);
+    double sc = (q75 - q25) / 1.3489795003921634;
+    if (fabs(sc) <= 1e-8) sc = 1.0;  // np.isclose(scale, 0) -> 1
+    locscale[blockIdx.x * 2] = (double)med;
+    locscale[blockIdx.x * 2 + 1] = sc;
+  }
 }
 
 template <typename F>
@@ -431,8 +632,8 @@ int spp_zero_dm(const float* in, float* out, int64_t nchans, int64_t nsamps, con
   if (!in || !out || !bpass || !chanwts) return fail(SPP_ERR_ARG, "null pointer");
   if (nchans <= 0 || nsamps < 0) return fail(SPP_ERR_ARG, "bad shape");
   if (nsamps == 0) return SPP_OK;
-  const unsigned blocks = (unsigned)std::min<int64_t>(nsamps, 148 * 16);
-  k_zero_dm<<<blocks, 256, 0, as_stream(stream)>>>(in, out, nchans, nsamps, bpass, chanwts);
+  const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(nsamps, kZdmRows), 148 * 6);
+  k_zero_dm<<<blocks, kZdmRows, 0, as_stream(stream)>>>(in, out, nchans, nsamps, bpass, chanwts);
   return cuda_status(cudaGetLastError(), "zero_dm launch");
 }
 
@@ -498,10 +699,12 @@ int64_t spp_boxcar_snr_workspace_bytes(int64_t nrows, int64_t n, int nfactors, i
   return snr_ws(nrows, n, nfactors, nwidths, &nck);
 }
 
-int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n, int64_t in_stride,
-                   const int32_t* factors, int nfactors, const int32_t* widths, int nwidths,
-                   float* snr, int32_t* peak_index, void* workspace, int64_t workspace_bytes,
-                   void* stream) {
+}  // extern "C"
+
+static int boxcar_snr_impl(const void* in, int in_kind, int64_t nrows, int64_t n,
+                           int64_t in_stride, const int32_t* factors, int nfactors,
+                           const int32_t* widths, int nwidths, float* snr, int32_t* peak_index,
+                           void* workspace, int64_t workspace_bytes, void* stream, bool robust) {
   if (!in || !factors || !widths || !snr || !workspace) return fail(SPP_ERR_ARG, "null pointer");
   if (in_kind != SPP_OUT_F32 && in_kind != SPP_OUT_I32) return fail(SPP_ERR_ARG, "bad in_kind");
   if (nrows <= 0 || n <= 0 || nfactors <= 0 || nfactors > 8 || nwidths <= 0 ||
@@ -522,7 +725,8 @@ int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n, int64_
     cfg.wmax = std::max(cfg.wmax, (int)widths[i]);
   }
   int64_t nck;
-  const int64_t need = snr_ws(nrows, n, nfactors, nwidths, &nck);
+  const int64_t base_need = snr_ws(nrows, n, nfactors, nwidths, &nck);
+  const int64_t need = base_need + (robust ? round_up(nrows * nfactors * 16, 256) : 0);
   if (workspace_bytes < need)
     return fail(SPP_ERR_SIZE, "workspace %lld < %lld", (long long)workspace_bytes, (long long)need);
   cudaStream_t st = as_stream(stream);
@@ -543,9 +747,64 @@ int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n, int64_
   k_snr_chunk<<<grid, kSnrThreads, smem, st>>>(in, in_kind, n, in_stride, cfg, nck, parts, stats);
   rc = cuda_status(cudaGetLastError(), "snr chunk launch");
   if (rc) return rc;
+  double* locscale = nullptr;
+  if (robust) {
+    locscale = reinterpret_cast<double*>(ws + base_need);
+    const int64_t qsmem = (int64_t)kQRanks * kQBins * 4;
+    rc = set_smem_attr(reinterpret_cast<const void*>(k_row_quantiles), qsmem);
+    if (rc) return rc;
+    k_row_quantiles<<<(unsigned)(nrows * nfactors), kQThreads, qsmem, st>>>(in, in_kind, n,
+                                                                          in_stride, cfg, locscale);
+    rc = cuda_status(cudaGetLastError(), "row quantiles launch");
+    if (rc) return rc;
+  }
   const int64_t nout = nrows * nfactors * nwidths;
-  k_snr_final<<<(unsigned)ceil_div(nout, 256), 256, 0, st>>>(n, cfg, nrows, nck, parts, stats, snr, peak_index);
+  k_snr_final<<<(unsigned)ceil_div(nout, 256), 256, 0, st>>>(n, cfg, nrows, nck, parts, stats, snr,
+                                                             peak_index, locscale);
   return cuda_status(cudaGetLastError(), "snr final launch");
+}
+
+extern "C" {
+
+int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n, int64_t in_stride,
+                   const int32_t* factors, int nfactors, const int32_t* widths, int nwidths,
+                   float* snr, int32_t* peak_index, void* workspace, int64_t workspace_bytes,
+                   void* stream) {
+  return boxcar_snr_impl(in, in_kind, nrows, n, in_stride, factors, nfactors, widths, nwidths, snr,
+                         peak_index, workspace, workspace_bytes, stream, false);
+}
+
+int spp_boxcar_filter(const float* in, int64_t n, int width, float* out, void* stream) {
+  if (!in || !out) return fail(SPP_ERR_ARG, "spp_boxcar_filter: null pointer");
+  if (width < 1) return fail(SPP_ERR_ARG, "invalid boxcar width: %d", width);
+  if (n <= 0) return fail(SPP_ERR_ARG, "empty series");
+  if (width > 8192) return fail(SPP_ERR_UNSUPPORTED, "boxcar width %d > 8192", width);
+  if (in == out) return fail(SPP_ERR_ARG, "spp_boxcar_filter: in and out must differ");
+  const int64_t pad_left = width / 2;
+  const int64_t ref_bin = (width % 2) ? -(width / 2) + 1 : -(width / 2);
+  const int64_t smem = (int64_t)(kBoxT + width - 1) * 4;
+  int rc = SPP_OK;
+  if (smem > 48 * 1024) {
+    rc = set_smem_attr(reinterpret_cast<const void*>(k_boxcar_filter), smem);
+    if (rc) return rc;
+  }
+  k_boxcar_filter<<<(unsigned)ceil_div(n, kBoxT), kBoxThreads, smem, as_stream(stream)>>>(
+      in, n, width, pad_left, ref_bin, out);
+  return cuda_status(cudaGetLastError(), "boxcar filter launch");
+}
+
+int64_t spp_boxcar_snr_robust_workspace_bytes(int64_t nrows, int64_t n, int nfactors,
+                                              int nwidths) {
+  int64_t nck;
+  return snr_ws(nrows, n, nfactors, nwidths, &nck) + round_up(nrows * nfactors * 16, 256);
+}
+
+int spp_boxcar_snr_robust(const void* in, int in_kind, int64_t nrows, int64_t n,
+                          int64_t in_stride, const int32_t* factors, int nfactors,
+                          const int32_t* widths, int nwidths, float* snr, int32_t* peak_index,
+                          void* workspace, int64_t workspace_bytes, void* stream) {
+  return boxcar_snr_impl(in, in_kind, nrows, n, in_stride, factors, nfactors, widths, nwidths, snr,
+                         peak_index, workspace, workspace_bytes, stream, true);
 }
 
 }  // extern "C"

@@ -140,11 +140,15 @@ class DMTPlan:
 
     mode "dedisperse": ``out[i][t] = sum_c x[t + D[i][c]][c]``, ``t < nsamps - max|D|``
     mode "roll":       ``out[i][t] = sum_c x[(t - D[i][c]) mod nsamps][c]``, ``t < nsamps``
+
+    Integer input is summed exactly.  Float32 input is summed in float64 in
+    channel order by default (``acc=ACC_F64``, the reference's accumulator);
+    ``ACC_KAHAN32`` trades that for compensated float32 slab sums.
     """
 
     def __init__(self, delays: np.ndarray, nchans: int, nsamps_max: int, *, nbits: int = 8,
                  bitorder: str = "big", mode: str = "dedisperse", out_dtype=torch.float32,
-                 acc: int = _lib.ACC_KAHAN32, device=None):
+                 acc: int = _lib.ACC_F64, device=None):
         delays = np.ascontiguousarray(np.atleast_2d(delays), dtype=np.int32)
         if delays.shape[1] != nchans:
             raise ValueError(f"delay table is {delays.shape}, expected (ndm, {nchans})")

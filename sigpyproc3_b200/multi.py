@@ -35,3 +35,9 @@ def max_over_ranks(value: float) -> float:
 
 def sum_over_ranks(value: float) -> float:
     return _reduce(value, dist.ReduceOp.SUM)
+
+
+def barrier() -> None:
+    """Barrier across ranks (no-op without an initialised process group)."""
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.barrier()

@@ -8,8 +8,6 @@ drop-in use.
 
 from __future__ import annotations
 
-import math
-
 import numpy as np
 import torch
 
@@ -70,24 +68,23 @@ class TimeSeries:
     def apply_boxcar(self, width: int) -> "TimeSeries":
         """Square-normalised running mean (timeseries.py:296-325): symmetric
         padding, moving mean of ``width``, times sqrt(width), rolled so the
-        reference bin matches the reference."""
+        reference bin matches the reference (one kernel, ``spp_boxcar_filter``;
+        window sums in float64)."""
         if width < 1:
             raise ValueError(f"invalid boxcar width: {width}")
-        x = self._cuda().to(torch.float64)
-        pad = (width // 2, width // 2) if width % 2 else (width // 2, width // 2 - 1)
-        n = x.numel()
-        left = x[: pad[0]].flip(0) if pad[0] else x[:0]
-        right = x[n - pad[1]:].flip(0) if pad[1] else x[:0]
-        xp = torch.cat([left, x, right])
-        c = torch.cat([torch.zeros(1, dtype=torch.float64, device=x.device), torch.cumsum(xp, 0)])
-        mean = (c[width:] - c[:-width]) / width
-        out = (mean * math.sqrt(width)).to(torch.float32)
-        ref_bin = -width // 2 + 1 if width % 2 else -width // 2
-        return TimeSeries(torch.roll(out, ref_bin), self.header.new_header())
+        x = self._cuda().contiguous()
+        out = torch.empty_like(x)
+        _lib.call("spp_boxcar_filter", x.data_ptr(), x.numel(), int(width), out.data_ptr(),
+                  stream_handle(None, x.device))
+        return TimeSeries(out, self.header.new_header())
 
-    def snr(self, widths=(1, 2, 4, 8, 16, 32, 64, 128, 256), factors=(1,)) -> np.ndarray:
-        """Boxcar S/N peaks of this series (see :func:`search.boxcar_snr`)."""
+    def snr(self, widths=(1, 2, 4, 8, 16, 32, 64, 128, 256), factors=(1,),
+            loc_scale: str = "mean_std") -> np.ndarray:
+        """Boxcar S/N peaks of this series (see :func:`search.boxcar_snr`);
+        ``loc_scale="median_iqr"`` z-scores with the median and the IQR, as
+        the reference MatchedFilter does by default."""
         from .search import boxcar_snr
 
-        snr, _ = boxcar_snr(self._cuda().view(1, -1), widths=widths, factors=factors)
+        snr, _ = boxcar_snr(self._cuda().view(1, -1), widths=widths, factors=factors,
+                            loc_scale=loc_scale)
         return snr[0].cpu().numpy()

@@ -20,9 +20,15 @@ def _events():
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def run(name: str, args, rank: int, world: int, local: int, emit) -> None:
-    {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "snr": run_snr,
-     "fold": run_fold}[name](args, rank, world, local, emit)
+def run(name: str, args, rank: int, world: int, local: int, emit, checks=None) -> None:
+    """Run one workload; ``checks`` maps a workload name to a correctness
+    checker the caller supplies (run outside the timed region)."""
+    fn = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "snr": run_snr,
+          "fold": run_fold}[name]
+    if name == "c5":
+        fn(args, rank, world, local, emit, checks or {})
+    else:
+        fn(args, rank, world, local, emit)
 
 
 def run_c1(args, rank, world, local, emit) -> None:
@@ -230,7 +236,7 @@ def measure_c3(steps: int, warmup: int, beams: int, batch: int, rank: int, world
     total_ms, units = 0.0, 0
     peaks = []
     torch.cuda.synchronize()
-    _barrier(world)
+    multi.barrier()
     for b0 in range(lo, hi, batch):
         blens = lens[b0:min(hi, b0 + batch)]
         srch = SubbandSearch(plan, blens, factors=factors, widths=widths, variants=best)
@@ -356,7 +362,7 @@ def run_c4(args, rank, world, local, emit) -> None:
              served_over_plain=stats["throughput"] / plain_value)
 
 
-def run_c5(args, rank, world, local, emit) -> None:
+def run_c5(args, rank, world, local, emit, checks=None) -> None:
     """Config 5: float32 4096 x 2^21, zero-DM, 4096 trials 0-3000, boxcar 1..512."""
     from .dedisp import DMTPlan, workspace
     from .search import boxcar_snr
@@ -372,10 +378,13 @@ def run_c5(args, rank, world, local, emit) -> None:
                nsamples=nsamps)
     nv = nsamps - int(d.max())
     out = torch.empty((ndm, nv), dtype=torch.float32, device="cuda")
-    # pick the accumulator and tile shape by timing one transform of each
-    # (--variant fixes a compensated-fp32 variant instead, for profiling)
+    # float64 channel-ordered sums (the reference's accumulator; the oracle's
+    # bits); --acc kahan selects the compensated float32 variants instead.
+    # The tile shape is picked by timing one transform of each variant
+    # (--variant fixes one, for profiling).
+    acc_sel = _lib.ACC_KAHAN32 if getattr(args, "acc", "f64") == "kahan" else _lib.ACC_F64
     tune = []
-    for acc in (_lib.ACC_KAHAN32, _lib.ACC_F64) if args.variant is None else ():
+    for acc in (acc_sel,) if args.variant is None else ():
         p = DMTPlan(d, g.nchans, nsamps, nbits=32, acc=acc)
         for v in range(p.num_variants):
             p.set_variant(v)
@@ -387,7 +396,7 @@ def run_c5(args, rank, world, local, emit) -> None:
             e1.synchronize()
             tune.append((e0.elapsed_time(e1), acc, v))
         p.close()
-    best = min(tune) if tune else (0.0, _lib.ACC_KAHAN32, args.variant)
+    best = min(tune) if tune else (0.0, acc_sel, args.variant)
     plan = DMTPlan(d, g.nchans, nsamps, nbits=32, acc=best[1])
     plan.set_variant(best[2])
     widths = tuple(1 << k for k in range(10))
@@ -414,11 +423,15 @@ def run_c5(args, rank, world, local, emit) -> None:
     tk = plan.timing_read()
     dmt_ms = tk["ms_dmt"] / max(tk["n"], 1)
     adds = ndm * nv * g.nchans
+    # per-result error against float64 sums, by the caller's checker (outside the timing)
+    checks = checks or {}
+    accuracy = checks["c5"](x, bp, out, d, g.nchans, nsamps) if "c5" in checks else None
     if rank == 0:
         emit(metric="DM-trial x samples/s, config 5 (float32 zero-DM + DM-time + boxcar S/N)",
              value=ndm * nv / (ms / 1e3), unit=UNIT, n_gpus=world, steps=args.steps, warmup=1,
              ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
-             dtype="f32 (fp32 slab partials, compensated sum across slabs)",
+             dtype="f32 in, f64 channel-ordered sums" if best[1] == _lib.ACC_F64 else
+                   "f32 (fp32 slab partials, compensated sum across slabs)",
              data="synthetic N(0,1) on device (seed 5)",
              config={"workload": f"config 5: float32 {g.nchans} ch x {nsamps}, zero-DM, {ndm} "
                      "trials 0-3000, boxcar widths 1..512", "tile": plan.describe(),
@@ -426,7 +439,7 @@ def run_c5(args, rank, world, local, emit) -> None:
                      "fp32 slab partials + Kahan across slabs",
                      "autotune_ms": [round(t[0], 2) for t in tune]},
              kernel_ms={"dmt": dmt_ms, "corner_turn_zero_dm": tk["ms_corner_turn"] / max(tk["n"], 1)},
-             fp32_adds_per_s=adds / (dmt_ms / 1e3), max_snr=float(snr.max()))
+             adds_per_s=adds / (dmt_ms / 1e3), max_snr=float(snr.max()), accuracy=accuracy)
     plan.close()
 
 

@@ -301,6 +301,17 @@ def main() -> None:
                            "input_sha256": sha(data_all)})
     meta["fold_cases"] = fold_cases
 
+    # ---- R9 robust z-score: np.median and the reference's _scale_iqr
+    # (core/stats.py:418-502, MatchedFilter's defaults) on seeded series
+    scale_iqr = refload.load_scale_iqr()
+    zs = []
+    rng = np.random.default_rng(17)
+    for k, m in enumerate((1, 2, 7, 8, 1000, 1001, 65536)):
+        y = (rng.normal(3.0, 2.0, m) if k % 2 else rng.integers(0, 9, m)).astype(np.float32)
+        out[f"zscore_in_{k}"] = y
+        zs.append({"m": m, "median": float(np.median(y)), "iqr_scale": float(scale_iqr(y))})
+    meta["zscore"] = zs
+
     # ---- N1 real files: Filterbank.dedisperse over the reference's sigproc
     # test files -- its read_plan block loop (readers.py:171-233), its
     # unpack kernels as FileReader.creadinto applies them (io/fileio.py:284-292,

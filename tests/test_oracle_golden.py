@@ -147,3 +147,31 @@ def test_py_floordiv_matches_python(orc):
         got = orc.lib().orc_py_floordiv(float(x), float(y))
         want = float(x) // float(y)
         assert got == want and math.copysign(1, got) == math.copysign(1, want), (x, y, got, want)
+
+
+def test_robust_zscore_matches_reference(orc, golden, golden_meta):
+    """median / IQR scale of the oracle equal np.median and the reference's
+    stats._scale_iqr (core/stats.py:480-502) on the recorded series."""
+    for k, rec in enumerate(golden_meta["zscore"]):
+        y = golden[f"zscore_in_{k}"]
+        loc, scale = orc.median_iqr(y)
+        assert loc == rec["median"], (k, loc, rec)
+        expect = rec["iqr_scale"] if not np.isclose(rec["iqr_scale"], 0) else 1.0
+        assert scale == expect, (k, scale, rec)
+
+
+def test_boxcar_snr_loc_scale_options(orc):
+    """The S/N oracle's two z-scores: mean/std and median/IQR."""
+    rng = np.random.default_rng(3)
+    x = rng.normal(10.0, 3.0, 5000).astype(np.float32)
+    x[2000:2010] += 20.0
+    s1, i1, l1, c1 = orc.boxcar_snr(x, (1, 2), (1, 4, 16), return_loc_scale=True)
+    s2, i2, l2, c2 = orc.boxcar_snr(x, (1, 2), (1, 4, 16), "median_iqr", return_loc_scale=True)
+    assert l1[0, 0] == pytest.approx(float(np.mean(x, dtype=np.float64)))
+    assert l2[0, 0] == float(np.median(x))
+    y2 = orc.downsample_mean(x, 2)
+    assert l2[0, 1] == float(np.median(y2))
+    q = np.percentile(y2.astype(np.float64), [25, 75])
+    assert c2[0, 1] == float((q[1] - q[0]) / 1.3489795003921634)
+    assert np.all(i1 == i2)  # same windows win; only the normalisation differs
+    assert np.all(s2 > 0) and np.all(s1 > 0)
