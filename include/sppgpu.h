@@ -230,6 +230,13 @@ int spp_collapse(const void* in, int nbits, int bitorder, int64_t nchans,
                  int64_t nsamps, float* tim, int64_t out_start, void* stream);
 int spp_zero_dm(const float* in, float* out, int64_t nchans, int64_t nsamps,
                 const float* bpass, const float* chanwts, void* stream);
+/* The same for uint8 input (8-bit files, Filterbank.remove_zerodm
+ * base.py:961-1028): each value stored as the low eight bits of the truncated
+ * float64 result, which is what the reference's numba cast to uint8 writes
+ * (the bandpass term is a channel sum, far above 255). */
+int spp_zero_dm_u8(const uint8_t* in, uint8_t* out, int64_t nchans,
+                   int64_t nsamps, const float* bpass, const float* chanwts,
+                   void* stream);
 
 /* ---- R8: downsample ----------------------------------------------------------
  * kernels.downsample_1d_mean (core/kernels.py:176-204): out[i] =
@@ -238,9 +245,16 @@ int spp_zero_dm(const float* in, float* out, int64_t nchans, int64_t nsamps,
 int spp_downsample_mean(const float* in, int64_t nrows, int64_t n,
                         int64_t in_stride, int factor, float* out,
                         int64_t out_stride, void* stream);
-/* kernels.downsample_2d_mean_flat (core/kernels.py:207-252) */
+/* kernels.downsample_2d_mean_flat (core/kernels.py:207-252): a dim1 x dim2
+ * row-major block (dim2 fastest) -> (dim1/factor1) x (dim2/factor2) means of
+ * factor1 x factor2 cells (float64 sums; the remainders dropped).  The _u8
+ * form keeps uint8 output as the reference does for 8-bit data (the mean
+ * truncated toward zero). */
 int spp_downsample_2d_mean(const float* in, int64_t dim1, int64_t dim2,
                            int factor1, int factor2, float* out, void* stream);
+int spp_downsample_2d_mean_u8(const uint8_t* in, int64_t dim1, int64_t dim2,
+                              int factor1, int factor2, uint8_t* out,
+                              void* stream);
 
 /* ---- R9: boxcar matched filter -> S/N peaks ------------------------------------
  * For each of `nrows` rows (row stride `in_stride` elements, `n` valid samples,

@@ -72,8 +72,10 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_bandpass": ([_p, _int, _int, _i64, _i64, _p, _p], _int),
     "spp_collapse": ([_p, _int, _int, _i64, _i64, _p, _i64, _p], _int),
     "spp_zero_dm": ([_p, _p, _i64, _i64, _p, _p, _p], _int),
+    "spp_zero_dm_u8": ([_p, _p, _i64, _i64, _p, _p, _p], _int),
     "spp_downsample_mean": ([_p, _i64, _i64, _i64, _int, _p, _i64, _p], _int),
     "spp_downsample_2d_mean": ([_p, _i64, _i64, _int, _int, _p, _p], _int),
+    "spp_downsample_2d_mean_u8": ([_p, _i64, _i64, _int, _int, _p, _p], _int),
     "spp_boxcar_snr_workspace_bytes": ([_i64, _i64, _int, _int], _i64),
     "spp_boxcar_snr": ([_p, _int, _i64, _i64, _i64, _p, _int, _p, _int, _p, _p, _p, _i64, _p],
                        _int),

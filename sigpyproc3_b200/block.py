@@ -76,6 +76,26 @@ class FilterbankBlock(BaseBlock):
     def get_tim(self) -> TimeSeries:
         return TimeSeries(self._t.sum(0), self.header.dedispersed_header(dm=self.dm))
 
+    def downsample(self, ffactor: int = 1, tfactor: int = 1,
+                   filter_method: str = "mean") -> "FilterbankBlock":
+        """Means over ``ffactor`` channels x ``tfactor`` samples (block.py:215-244,
+        stats.downsample_2d core/stats.py:96-136), remainders dropped, on the
+        GPU (float64 sums; the reference averages in float32, so results can
+        differ in the last bit for non-integer data)."""
+        if filter_method != "mean":
+            raise NotImplementedError("only filter_method='mean' runs on the GPU")
+        if not all(isinstance(f, int) and f > 0 for f in (ffactor, tfactor)):
+            raise ValueError("Factors must be positive integers.")
+        x = self._t.contiguous()
+        nch, n = x.shape
+        out = torch.empty((nch // ffactor, n // tfactor), dtype=torch.float32, device=x.device)
+        _lib.call("spp_downsample_2d_mean", x.data_ptr(), nch, n, ffactor, tfactor,
+                  out.data_ptr(), torch.cuda.current_stream(x.device).cuda_stream)
+        changes = {"tsamp": self.header.tsamp * tfactor, "foff": self.header.foff * ffactor,
+                   "nsamples": self.header.nsamples // tfactor,
+                   "nchans": self.header.nchans // ffactor}
+        return FilterbankBlock(out, self.header.new_header(changes))
+
     def get_bandpass(self) -> np.ndarray:
         return self._t.sum(1).cpu().numpy()
 

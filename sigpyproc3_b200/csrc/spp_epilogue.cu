@@ -64,9 +64,19 @@ __global__ void k_collapse(const void* __restrict__ in, int64_t nchans, int64_t 
 // a block of 8 warps takes 256 samples; each warp sums 32 samples' channels in
 // channel order (32 x 32 tiles staged through shared memory, one lane per
 // sample), then the block rewrites the 256 spectra with coalesced accesses.
+// The result is stored in the input's type: float32 rounds; uint8 keeps the low
+// eight bits of the truncated value (what the reference's numba cast of a
+// float64 to uint8 yields on x86, where values far above 255 are the norm
+// because the bandpass is a channel sum).
+__device__ __forceinline__ float zdm_store(float, double v) { return (float)v; }
+__device__ __forceinline__ uint8_t zdm_store(uint8_t, double v) {
+  return (uint8_t)(uint64_t)(int64_t)v;
+}
+
 constexpr int kZdmRows = 256;
+template <typename T>
 __global__ void __launch_bounds__(kZdmRows)
-k_zero_dm(const float* __restrict__ in, float* __restrict__ out, int64_t nchans, int64_t nsamps,
+k_zero_dm(const T* __restrict__ in, T* __restrict__ out, int64_t nchans, int64_t nsamps,
           const float* __restrict__ bpass, const float* __restrict__ chanwts) {
   __shared__ float tile[kZdmRows / 32][32][33];
   __shared__ double zs[kZdmRows];
@@ -78,7 +88,7 @@ k_zero_dm(const float* __restrict__ in, float* __restrict__ out, int64_t nchans,
       const int64_t c = c0 + lane;
       for (int r = 0; r < 32; ++r) {
         const int64_t t = t0 + r;
-        tile[warp][r][lane] = (t < nsamps && c < nchans) ? __ldg(in + t * nchans + c) : 0.f;
+        tile[warp][r][lane] = (t < nsamps && c < nchans) ? (float)in[t * nchans + c] : 0.f;
       }
       __syncwarp();
       const int nc = (nchans - c0) < 32 ? (int)(nchans - c0) : 32;
@@ -90,12 +100,12 @@ k_zero_dm(const float* __restrict__ in, float* __restrict__ out, int64_t nchans,
     const int64_t rows = imin64(kZdmRows, nsamps - tb);
     for (int64_t r = 0; r < rows; ++r) {
       const double z = zs[r];
-      const float* src = in + (tb + r) * nchans;
-      float* dst = out + (tb + r) * nchans;
+      const T* src = in + (tb + r) * nchans;
+      T* dst = out + (tb + r) * nchans;
       for (int64_t c = threadIdx.x; c < nchans; c += kZdmRows) {
         const double t1 = __dmul_rn(z, (double)chanwts[c]);
         const double t2 = __dsub_rn((double)src[c], t1);
-        dst[c] = (float)__dadd_rn(t2, (double)bpass[c]);
+        dst[c] = zdm_store(T(), __dadd_rn(t2, (double)bpass[c]));
       }
     }
     __syncthreads();
@@ -157,8 +167,14 @@ __global__ void k_downsample(const float* __restrict__ in, int64_t n, int64_t in
 }
 
 // downsample_2d_mean_flat
-__global__ void k_downsample_2d(const float* __restrict__ in, int64_t dim1, int64_t dim2,
-                                int f1, int f2, float* __restrict__ out) {
+__device__ __forceinline__ float ds_store(float, double v) { return (float)v; }
+__device__ __forceinline__ uint8_t ds_store(uint8_t, double v) {
+  return (uint8_t)(uint64_t)(int64_t)v;  // numba's float64 -> uint8 cast (truncation)
+}
+
+template <typename T>
+__global__ void k_downsample_2d(const T* __restrict__ in, int64_t dim1, int64_t dim2,
+                                int f1, int f2, T* __restrict__ out) {
   const int64_t n1 = dim1 / f1, n2 = dim2 / f2;
   const int64_t total = n1 * n2;
   const double tot = (double)f1 * f2;
@@ -169,7 +185,7 @@ __global__ void k_downsample_2d(const float* __restrict__ in, int64_t dim1, int6
     const int64_t pos = dim2 * i * f1 + j * f2;
     for (int a = 0; a < f1; ++a)
       for (int b = 0; b < f2; ++b) s += (double)in[pos + a * dim2 + b];
-    out[idx] = (float)(s / tot);
+    out[idx] = ds_store(T(), s / tot);
   }
 }
 
@@ -633,7 +649,19 @@ int spp_zero_dm(const float* in, float* out, int64_t nchans, int64_t nsamps, con
   if (nchans <= 0 || nsamps < 0) return fail(SPP_ERR_ARG, "bad shape");
   if (nsamps == 0) return SPP_OK;
   const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(nsamps, kZdmRows), 148 * 6);
-  k_zero_dm<<<blocks, kZdmRows, 0, as_stream(stream)>>>(in, out, nchans, nsamps, bpass, chanwts);
+  k_zero_dm<float><<<blocks, kZdmRows, 0, as_stream(stream)>>>(in, out, nchans, nsamps, bpass,
+                                                               chanwts);
+  return cuda_status(cudaGetLastError(), "zero_dm launch");
+}
+
+int spp_zero_dm_u8(const uint8_t* in, uint8_t* out, int64_t nchans, int64_t nsamps,
+                   const float* bpass, const float* chanwts, void* stream) {
+  if (!in || !out || !bpass || !chanwts) return fail(SPP_ERR_ARG, "null pointer");
+  if (nchans <= 0 || nsamps < 0) return fail(SPP_ERR_ARG, "bad shape");
+  if (nsamps == 0) return SPP_OK;
+  const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(nsamps, kZdmRows), 148 * 6);
+  k_zero_dm<uint8_t><<<blocks, kZdmRows, 0, as_stream(stream)>>>(in, out, nchans, nsamps, bpass,
+                                                                 chanwts);
   return cuda_status(cudaGetLastError(), "zero_dm launch");
 }
 
@@ -657,7 +685,19 @@ int spp_downsample_2d_mean(const float* in, int64_t dim1, int64_t dim2, int fact
   const int64_t total = (dim1 / factor1) * (dim2 / factor2);
   if (total == 0) return SPP_OK;
   const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(total, 256), 148 * 32);
-  k_downsample_2d<<<blocks, 256, 0, as_stream(stream)>>>(in, dim1, dim2, factor1, factor2, out);
+  k_downsample_2d<float><<<blocks, 256, 0, as_stream(stream)>>>(in, dim1, dim2, factor1, factor2, out);
+  return cuda_status(cudaGetLastError(), "downsample_2d launch");
+}
+
+int spp_downsample_2d_mean_u8(const uint8_t* in, int64_t dim1, int64_t dim2, int factor1,
+                              int factor2, uint8_t* out, void* stream) {
+  if (!in || !out) return fail(SPP_ERR_ARG, "null pointer");
+  if (factor1 <= 0 || factor2 <= 0 || dim1 < 0 || dim2 < 0) return fail(SPP_ERR_ARG, "bad factors");
+  const int64_t total = (dim1 / factor1) * (dim2 / factor2);
+  if (total == 0) return SPP_OK;
+  const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(total, 256), 148 * 32);
+  k_downsample_2d<uint8_t><<<blocks, 256, 0, as_stream(stream)>>>(in, dim1, dim2, factor1, factor2,
+                                                                  out);
   return cuda_status(cudaGetLastError(), "downsample_2d launch");
 }
 

@@ -131,3 +131,12 @@ class Header:
 
     def write_sigproc(self, path, data) -> None:
         sigproc.write_filterbank(path, self.to_sigproc_dict(), data)
+
+    def prep_outfile(self, filename, *, updates: dict | None = None,
+                     nbits: int | None = None) -> sigproc.SigprocWriter:
+        """A sigproc file with this header (plus ``updates``) written, ready for
+        data blocks (header.py:575-619)."""
+        nbits = self.nbits if nbits is None else int(nbits)
+        upd = dict(updates or {})
+        upd["nbits"] = nbits
+        return sigproc.SigprocWriter(filename, self.new_header(upd).to_sigproc_dict(), nbits)

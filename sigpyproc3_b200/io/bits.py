@@ -70,3 +70,20 @@ def unpack(packed, nbits: int, bitorder: str = "big", out=None, stream=None):
     _lib.call("spp_unpack", packed.data_ptr(), n, nbits, bitorder_code(bitorder), out.data_ptr(),
               st.cuda_stream)
     return out
+
+
+def pack_host(vals: np.ndarray, nbits: int, bitorder: str = "big") -> np.ndarray:
+    """Pack uint8 samples (one per byte) into nbits-wide fields, ``8 // nbits``
+    per byte in the reference's layout (kernels.pack{1,2,4}_8_{big,little},
+    core/kernels.py:72-173): sample k of a byte sits in the high bits first
+    for big order, in the low bits first for little order.  Host-side: it
+    serves file writing, not the GPU path."""
+    if nbits not in (1, 2, 4):
+        raise ValueError(f"pack: nbits must be 1, 2 or 4 (got {nbits})")
+    per = 8 // nbits
+    v = np.ascontiguousarray(vals, dtype=np.uint8).reshape(-1, per)
+    out = np.zeros(v.shape[0], dtype=np.uint8)
+    for k in range(per):
+        sh = (8 - (k + 1) * nbits) if bitorder == "big" else k * nbits
+        out |= (v[:, k] << np.uint8(sh)).astype(np.uint8)
+    return out

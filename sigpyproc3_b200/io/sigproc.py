@@ -154,3 +154,35 @@ def write_filterbank(path: str | Path, hdr: dict, data) -> None:
     with Path(path).open("wb") as fp:
         fp.write(encode_header(hdr))
         fp.write(np.ascontiguousarray(data).tobytes())
+
+
+class SigprocWriter:
+    """Incremental sigproc writer: the header first, then data blocks
+    appended in order (the role of the reference's FileWriter, io/fileio.py:
+    346-412, without its optional rescaling).  Samples of nbits < 8 arrive as
+    one uint8 per sample and are packed in the reference's bit order."""
+
+    def __init__(self, path: str | Path, hdr: dict, nbits: int):
+        self.path = Path(path)
+        self.nbits = int(nbits)
+        self._fp = self.path.open("wb")
+        self._fp.write(encode_header(hdr))
+
+    def cwrite(self, arr) -> None:
+        import numpy as np
+
+        from .bits import DEFAULT_BITORDER, pack_host
+
+        a = np.ascontiguousarray(arr)
+        if self.nbits in (1, 2, 4):
+            a = pack_host(a, self.nbits, DEFAULT_BITORDER[self.nbits])
+        self._fp.write(a.tobytes())
+
+    def close(self) -> None:
+        self._fp.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -264,6 +264,125 @@ class Filterbank:
             tim /= h.nchans
         return TimeSeries(tim, h.new_header({"nchans": 1, "dm": 0}))
 
+    # --- file-writing operations (R7, R10, N2) ---
+    def _block_values(self, raw: torch.Tensor, nsamps_r: int) -> torch.Tensor:
+        """The block's samples in the reference's read_plan dtype: one uint8 per
+        sample (packed data unpacked on the GPU) or float32."""
+        h = self.header
+        raw = raw[: nsamps_r * self.row_bytes]
+        if h.nbits in (1, 2, 4):
+            return gpu_unpack(raw, h.nbits, self.bitorder)
+        if h.nbits == 32:
+            return raw.view(torch.float32)
+        return raw
+
+    def remove_zerodm(self, outfile_name: str | None = None, gulp: int = 16384, start: int = 0,
+                      nsamps: int | None = None, *, parallel: bool = False,
+                      **plan_kwargs) -> str:
+        """Remove the channel-weighted zero-DM signal and write a new file
+        (base.py:961-1028; Eatough, Keane & Lyne 2009).
+
+        As the reference: the bandpass is the sum over the whole file
+        (``self.bandpass(**plan_kwargs)``), ``chanwts = bpass / sum(bpass)``
+        in float32, and each block becomes ``x - zdm * chanwts + bpass``
+        (float64, zdm the channel sum of the spectrum) in the file's own
+        sample format: float32 rounded, 8-bit as the low eight bits of the
+        truncated value (the reference's uint8 cast), 1/2/4-bit repacked."""
+        del parallel
+        h = self.header
+        if outfile_name is None:
+            outfile_name = f"{h.basename}_noZeroDM.fil"
+        bp = self.bandpass(**plan_kwargs).data
+        chanwts = (bp / bp.sum()).astype(np.float32)
+        dev = torch.device("cuda", torch.cuda.current_device())
+        bp_d = torch.from_numpy(bp).to(dev)
+        w_d = torch.from_numpy(chanwts).to(dev)
+        st = stream_handle(None, dev)
+        with h.prep_outfile(outfile_name, nbits=h.nbits) as out_file:
+            for nsamps_r, _ii, raw in self.stream_blocks(gulp, start, nsamps, **plan_kwargs):
+                x = self._block_values(raw, nsamps_r)
+                y = torch.empty_like(x)
+                fn = "spp_zero_dm" if h.nbits == 32 else "spp_zero_dm_u8"
+                _lib.call(fn, x.data_ptr(), y.data_ptr(), h.nchans, nsamps_r, bp_d.data_ptr(),
+                          w_d.data_ptr(), st)
+                out_file.cwrite(y.cpu().numpy())
+        return outfile_name
+
+    def downsample(self, tfactor: int = 1, ffactor: int = 1, outfile_name: str | None = None,
+                   gulp: int = 16384, start: int = 0, nsamps: int | None = None, *,
+                   compat: bool = False, **plan_kwargs) -> str:
+        """Decimate in time and frequency and write a new file (base.py:585-654):
+        means of ``tfactor`` samples x ``ffactor`` channels (float64 sums,
+        kernels.downsample_2d_mean_flat core/kernels.py:207-252), in the
+        file's sample format (8-bit and packed means truncated to integers),
+        header tsamp * tfactor, nchans // ffactor, foff * ffactor.
+
+        The reference's block loop passes (nchans, nsamps) where the kernel
+        expects (samples, channels) of its time-major block, which averages
+        across the wrong axes; ``compat=True`` repeats that call exactly,
+        the default averages as documented."""
+        h = self.header
+        if outfile_name is None:
+            outfile_name = f"{h.basename}_f{ffactor:d}_t{tfactor:d}.fil"
+        if h.nchans % ffactor != 0:
+            raise ValueError(f"Bad frequency factor given: {ffactor:d}")
+        if tfactor < 1 or ffactor < 1:
+            raise ValueError("Factors must be positive integers.")
+        gulp = int(np.ceil(gulp / tfactor) * tfactor)
+        updates = {"tsamp": h.tsamp * tfactor, "nchans": h.nchans // ffactor,
+                   "foff": h.foff * ffactor}
+        st = stream_handle(None, torch.device("cuda", torch.cuda.current_device()))
+        with h.prep_outfile(outfile_name, updates=updates) as out_file:
+            for nsamps_r, _ii, raw in self.stream_blocks(gulp, start, nsamps, **plan_kwargs):
+                x = self._block_values(raw, nsamps_r)
+                dims = (h.nchans, nsamps_r) if compat else (nsamps_r, h.nchans)
+                fac = (tfactor, ffactor)
+                y = torch.empty((dims[0] // fac[0]) * (dims[1] // fac[1]), dtype=x.dtype,
+                                device=x.device)
+                fn = "spp_downsample_2d_mean" if h.nbits == 32 else "spp_downsample_2d_mean_u8"
+                _lib.call(fn, x.data_ptr(), dims[0], dims[1], fac[0], fac[1], y.data_ptr(), st)
+                out_file.cwrite(y.cpu().numpy())
+        return outfile_name
+
+    def subband(self, dm: float, nsub: int, ref_freq: str | float = "fch1",
+                outfile_name: str | None = None, gulp: int = 16384, start: int = 0,
+                nsamps: int | None = None, **plan_kwargs) -> str:
+        """Dedisperse into ``nsub`` subbands at one DM and write them as a
+        32-bit file (base.py:1030-1107): channel c goes to subband
+        ``c // (nchans // nsub)``, the read_plan blocks overlap by the maximum
+        delay, header fch1 = ftop - new_foff / 2, foff = foff * nchans // nsub,
+        refdm = dm, nchans = nsub.  Each block's sums start from zero (the
+        reference never clears its output buffer between blocks)."""
+        h = self.header
+        subfactor = h.nchans // nsub
+        chan_delays = np.atleast_1d(h.get_dmdelays(dm, ref_freq)).astype(np.int32)
+        max_delay = int(np.max(np.abs(chan_delays)))
+        gulp = max(2 * max_delay, gulp)
+        new_foff = h.foff * h.nchans // nsub
+        new_fch1 = h.ftop - new_foff / 2
+        chan_to_sub = (np.arange(h.nchans, dtype=np.int32) // subfactor).astype(np.int32)
+        if chan_to_sub.max() >= nsub:
+            raise ValueError(f"nchans ({h.nchans}) is not a multiple of nsub ({nsub})")
+        updates = {"fch1": new_fch1, "foff": new_foff, "refdm": dm, "nchans": nsub}
+        if outfile_name is None:
+            outfile_name = f"{h.basename}_DM{dm:06.2f}.subbands"
+        dev = torch.device("cuda", torch.cuda.current_device())
+        d_d = torch.from_numpy(chan_delays).to(dev)
+        c_d = torch.from_numpy(chan_to_sub).to(dev)
+        st = stream_handle(None, dev)
+        with h.prep_outfile(outfile_name, updates=updates, nbits=32) as out_file:
+            for nsamps_r, _ii, raw in self.stream_blocks(gulp, start, nsamps,
+                                                        skipback=max_delay, **plan_kwargs):
+                nout = nsamps_r - max_delay
+                if nout <= 0:
+                    continue
+                y = torch.empty(nout * nsub, dtype=torch.float32, device=dev)
+                _lib.call("spp_subband", raw.data_ptr(), h.nbits, bitorder_code(self.bitorder),
+                          h.nchans, nsamps_r, d_d.data_ptr(), max_delay, c_d.data_ptr(), nsub,
+                          y.data_ptr(), st)
+                out_file.cwrite(y.cpu().numpy())
+        return outfile_name
+
     # --- N4: folding ---
     def fold(self, period: float, dm: float, accel: float = 0, nbins: int = 50, nints: int = 32,
              nbands: int = 32, gulp: int = 16384, start: int = 0, nsamps: int | None = None,

@@ -312,6 +312,57 @@ def main() -> None:
         zs.append({"m": m, "median": float(np.median(y)), "iqr_scale": float(scale_iqr(y))})
     meta["zscore"] = zs
 
+    # ---- N2 kernels.downsample_2d_mean_flat (core/kernels.py:207-252) on
+    # time-major blocks (dim1 = samples, dim2 = channels): uint8 (the mean is
+    # cast back to uint8) and float32
+    rng = np.random.default_rng(18)
+    for tag, arr in (("u8", rng.integers(0, 256, size=(1001, 48), dtype=np.uint8)),
+                     ("f32", rng.normal(0.0, 1.0, size=(1001, 48)).astype(np.float32))):
+        out[f"ds2d_{tag}_in"] = arr
+        for f1, f2 in ((3, 2), (4, 4), (1, 8), (7, 1)):
+            out[f"ds2d_{tag}_{f1}_{f2}"] = K.downsample_2d_mean_flat(arr.ravel(), f1, f2, 1001, 48)
+
+    # ---- N2/R10 file operations through their block loops:
+    # Filterbank.remove_zerodm (base.py:961-1028: bandpass over the whole file,
+    # then kernels.remove_zerodm per read_plan block, output in the input's
+    # dtype) and Filterbank.downsample's per-block kernel call exactly as
+    # base.py:644-653 makes it (dims passed as (nchans, nsamps_r))
+    fops = {}
+    for tag, nbits, nch, nsamples, seed in (("u8", 8, 64, 5000, 31), ("f32", 32, 48, 3000, 33)):
+        rng = np.random.default_rng(seed)
+        if nbits == 32:
+            vals = rng.normal(5.0, 2.0, nsamples * nch).astype(np.float32)
+        else:
+            vals = rng.integers(0, 256, nsamples * nch, dtype=np.uint8)
+        isz = vals.dtype.itemsize
+        gulp = 1000
+
+        def reader():
+            fr = FakeReader(vals.view(np.uint8), nsamples, nch, isz)
+            fr.bitsinfo.dtype = vals.dtype
+            return fr
+
+        bp = np.zeros(nch, dtype=np.float32)
+        for nsamps_r, _ii, data in read_plan(reader(), gulp=16384, quiet=True):
+            K.extract_bpass(np.ascontiguousarray(data), bp, nch, nsamps_r)
+        zparts = []
+        for nsamps_r, _ii, data in read_plan(reader(), gulp=gulp, quiet=True):
+            o = np.empty(nsamps_r * nch, dtype=vals.dtype)
+            K.remove_zerodm(np.ascontiguousarray(data), o, bp, nch, nsamps_r)
+            zparts.append(o)
+        out[f"fop_{tag}_zerodm"] = np.concatenate(zparts)
+        out[f"fop_{tag}_zerodm_bpass"] = bp
+        tf, ff = 4, 2
+        g2 = int(np.ceil(gulp / tf) * tf)
+        dparts = []
+        for nsamps_r, _ii, data in read_plan(reader(), gulp=g2, quiet=True):
+            dparts.append(K.downsample_2d_mean_flat(np.ascontiguousarray(data), tf, ff, nch,
+                                                    nsamps_r))
+        out[f"fop_{tag}_downsample_compat"] = np.concatenate(dparts)
+        fops[tag] = {"nbits": nbits, "nchans": nch, "nsamples": nsamples, "gulp": gulp,
+                     "tfactor": tf, "ffactor": ff, "seed": seed, "input_sha256": sha(vals)}
+    meta["file_ops"] = fops
+
     # ---- N1 real files: Filterbank.dedisperse over the reference's sigproc
     # test files -- its read_plan block loop (readers.py:171-233), its
     # unpack kernels as FileReader.creadinto applies them (io/fileio.py:284-292,

@@ -214,3 +214,27 @@ def test_host_twins_follow_the_generator_definitions():
                                   synth_host.gauss_u8_thresholds(96.0, 12.0))
     x = synth_host.c2_filterbank_host(199_990, 40)
     assert x.shape == (40, 1024) and x.dtype == np.uint8
+
+
+@pytest.mark.parametrize("nbits,order", [(1, "little"), (1, "big"), (2, "big"), (2, "little"),
+                                         (4, "big"), (4, "little")])
+def test_pack_host_inverts_unpack(orc, nbits, order):
+    """Host packing for written files: the inverse of the reference's unpack."""
+    from sigpyproc3_b200.io.bits import pack_host
+
+    raw = np.random.default_rng(nbits).integers(0, 256, 999, dtype=np.uint8)
+    np.testing.assert_array_equal(pack_host(orc.unpack(raw, nbits, order), nbits, order), raw)
+
+
+def test_sigproc_writer_roundtrip(tmp_path):
+    from sigpyproc3_b200 import Header
+    from sigpyproc3_b200.io import sigproc
+
+    h = Header(nchans=16, nbits=2, nsamples=0, fch1=1400.0, foff=-2.0, tsamp=1e-3,
+               filename=str(tmp_path / "a.fil"))
+    vals = np.random.default_rng(1).integers(0, 4, 16 * 40, dtype=np.uint8)
+    with h.prep_outfile(tmp_path / "w.fil", updates={"foff": -4.0}) as w:
+        w.cwrite(vals[:320])
+        w.cwrite(vals[320:])
+    hdr = sigproc.read_header(tmp_path / "w.fil")
+    assert hdr["nsamples"] == 40 and hdr["foff"] == -4.0 and hdr["nbits"] == 2
