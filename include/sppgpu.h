@@ -280,7 +280,8 @@ int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n,
  * "mean" (core/stats.py:200-243): out[(i + ref_bin) mod n] = f32(sqrt(w) *
  * mean(p[i .. i+w-1])), p = the n samples padded symmetrically (np.pad
  * "symmetric") by w/2 on the left and w/2 (odd w) or w/2-1 (even w) on the
- * right, ref_bin = -w/2 + 1 (odd w) or -w/2 (even w).  Window sums in float64
+ * right, ref_bin = -floor(w/2) (the reference's -w // 2 + 1 for odd w, -w // 2
+ * for even w, in Python floor division).  Window sums in float64
  * (the reference's bottleneck.move_mean keeps a float32 running sum).
  * 1 <= width <= 8192; `in` and `out` distinct device arrays of n floats. */
 int spp_boxcar_filter(const float* in, int64_t n, int width, float* out,

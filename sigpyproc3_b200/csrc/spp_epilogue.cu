@@ -821,7 +821,9 @@ int spp_boxcar_filter(const float* in, int64_t n, int width, float* out, void* s
   if (width > 8192) return fail(SPP_ERR_UNSUPPORTED, "boxcar width %d > 8192", width);
   if (in == out) return fail(SPP_ERR_ARG, "spp_boxcar_filter: in and out must differ");
   const int64_t pad_left = width / 2;
-  const int64_t ref_bin = (width % 2) ? -(width / 2) + 1 : -(width / 2);
+  // the reference's -width // 2 + 1 (odd) or -width // 2 (even), Python floor
+  // division: -(width / 2) either way
+  const int64_t ref_bin = -(int64_t)(width / 2);
   const int64_t smem = (int64_t)(kBoxT + width - 1) * 4;
   int rc = SPP_OK;
   if (smem > 48 * 1024) {

@@ -272,6 +272,15 @@ k_dedisp_single8_hd(const __grid_constant__ S2Args<NS> a) {
   extern __shared__ __align__(16) uint8_t sm[];
   const int T = 4 * G * (int)(blockDim.x >> 5);
   const int64_t t0 = (int64_t)blockIdx.x * T;
+  // channel offsets into shared memory (each lane reads the four of its word);
+  // kernel parameters only, so this runs before the wait below
+  int32_t* tab = reinterpret_cast<int32_t*>(sm + a.tab_off);
+  for (int c = threadIdx.x; c < 32 * a.nslab; c += blockDim.x) tab[c] = a.off[c];
+  // Programmatic dependent launch: the previous kernel in the stream may still
+  // be finishing (this grid was allowed to launch early); wait until its
+  // memory operations are complete and visible before reading the input or
+  // writing the output.  Without the launch attribute this returns at once.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     if (s < a.nslab)
@@ -279,9 +288,9 @@ k_dedisp_single8_hd(const __grid_constant__ S2Args<NS> a) {
                a.nrows[s], 32 * s);
     cp_async_commit();  // one group per slab (empty past nslab)
   }
-  // channel offsets into shared memory (each lane reads the four of its word)
-  int32_t* tab = reinterpret_cast<int32_t*>(sm + a.tab_off);
-  for (int c = threadIdx.x; c < 32 * a.nslab; c += blockDim.x) tab[c] = a.off[c];
+  // the next kernel in the stream may start launching (it waits for this
+  // grid's completion before touching memory)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = lane & 3, j = lane >> 2;
   const int obase = warp * 4 * G + i;  // this lane's first output row within the CTA
@@ -392,8 +401,17 @@ static int launch_hd(const uint8_t* raw, int64_t nchans, int64_t nsamps, const i
   if (rc) return rc;
   const int64_t gx = ceil_div(nvalid, T);
   if (gx > INT32_MAX || nsamps > INT32_MAX) return SPP_ERR_UNSUPPORTED;
-  fn<<<(unsigned)gx, 32 * W, smem, st>>>(a);
-  return cuda_status(cudaGetLastError(), "single-DM (host table) launch");
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)gx);
+  cfg.blockDim = dim3(32 * W);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cuda_status(cudaLaunchKernelEx(&cfg, fn, a), "single-DM (host table) launch");
 }
 
 // 8-bit, nchans a multiple of 32 up to 1024, delays in host memory; returns

@@ -80,9 +80,11 @@ def test_zero_dm_dmt_float(orc, acc):
 
 
 def test_config5_geometry(orc):
-    """4096 channels of N(0, 1) float32 at the config-5 band, 24 trials spread
-    over DM 0-3000 plus the 8 highest, a window of 8192 outputs past the
-    48 602-sample maximum delay, zero-DM fused.  The default (float64)
+    """4096 channels of N(0, 1) float32 at the config-5 band, three blocks of
+    16 adjacent trials of the dmt_transform(1500, 4096) grid (DM 0-12,
+    ~1494-1506 and ~2988-3000; adjacent trials, as in the full grid, keep a
+    DM tile's delay spread within shared memory), a window of 8192 outputs past
+    the 48 602-sample maximum delay, zero-DM fused.  The default (float64)
     accumulator reproduces the oracle's bits; the compensated float32 one is
     held to its documented bound, and both report their per-result error
     against the float64 sums."""
@@ -90,24 +92,29 @@ def test_config5_geometry(orc):
     from sigpyproc3_b200.dedisp import DMTPlan
 
     grid = synth.dm_grid(1500.0, 4096)
-    dms = np.concatenate([grid[np.linspace(0, 4095, 24).astype(int)], grid[-8:]])
     nchans = 4096
     nsamps = 8192 + 48602
-    d, x, bp, w, y, ref32, ref64, nv = _zero_dm_case(orc, nchans, nsamps, synth.C5.foff, dms)
-    assert int(d.max()) == 48602 and nv == 8192
-    mag = orc.dmt(np.abs(y), d, nchans, nsamps, nv).astype(np.float64)
+    top = grid[-16:]
+    d_top, x, bp, w, y, ref32, ref64, nv = _zero_dm_case(orc, nchans, nsamps, synth.C5.foff, top)
+    assert int(d_top.max()) == 48602 and nv == 8192
     reports = {}
-    for acc in (_lib.ACC_F64, _lib.ACC_KAHAN32):
-        plan = DMTPlan(d, nchans, nsamps, nbits=32, acc=acc)
-        for v in range(plan.num_variants):
-            plan.set_variant(v)
-            out = plan.execute_zero_dm(x, nsamps, bp, w).cpu().numpy()
-            rep = error_report(out, ref64, mag)
-            reports[(acc, v)] = rep
-            if acc == _lib.ACC_F64:
-                np.testing.assert_array_equal(out, ref32, err_msg=str(plan.describe()))
-                assert rep["frac_beyond_rtol"] == 0.0, rep
-            else:
-                assert rep["max_err_over_bound"] <= 1.0, (v, rep)
-        plan.close()
+    for name, block in (("bottom", grid[:16]), ("middle", grid[2040:2056]), ("top", top)):
+        d = np.atleast_2d(synth.C5.delays(block)).astype(np.int32)
+        r32, r64 = orc.dmt(y, d, nchans, nsamps, nv, want64=True)
+        mag = orc.dmt(np.abs(y), d, nchans, nsamps, nv).astype(np.float64)
+        for acc in (_lib.ACC_F64, _lib.ACC_KAHAN32):
+            plan = DMTPlan(d, nchans, nsamps, nbits=32, acc=acc)
+            out_full = None
+            for v in range(plan.num_variants):
+                plan.set_variant(v)
+                out_full = plan.execute_zero_dm(x, nsamps, bp, w).cpu().numpy()
+                out = out_full[:, :nv]
+                rep = error_report(out, r64, mag)
+                reports[(name, acc, v)] = rep
+                if acc == _lib.ACC_F64:
+                    np.testing.assert_array_equal(out, r32, err_msg=str(plan.describe()))
+                    assert rep["frac_beyond_rtol"] == 0.0, rep
+                else:
+                    assert rep["max_err_over_bound"] <= 1.0, (v, rep)
+            plan.close()
     print("per-result error vs float64:", reports)
