@@ -129,6 +129,17 @@ int spp_fold(const void* in, int nbits, int64_t nchans, int64_t nsamps,
              float accel, int64_t total_nsamps, int32_t nbins, int32_t nints,
              int32_t nsubs, int64_t index, const int32_t* band_start, float* fold_ar,
              int32_t* count_ar, int64_t cells, void* stream);
+/* The 8-bit form with exact cells: fold_sums holds 64-bit integer sums (the
+ * caller converts them to float32 once at the end), so the result is exact and
+ * independent of the order of the atomic adds for any observation length.
+ * The reference's float32 cells (sequential adds) equal it while every cell
+ * stays below 2^24. */
+int spp_fold_exact(const void* in, int64_t nchans, int64_t nsamps,
+                   const int32_t* delays, int32_t maxdelay, float tsamp,
+                   float period, float accel, int64_t total_nsamps,
+                   int32_t nbins, int32_t nints, int32_t nsubs, int64_t index,
+                   const int32_t* band_start, unsigned long long* fold_sums,
+                   int32_t* count_ar, int64_t cells, void* stream);
 
 /* Same computation as spp_dedisperse, but allocating nothing and taking no
  * workspace.  No counterpart in the reference.  It serves callers that must not

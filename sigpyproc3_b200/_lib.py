@@ -50,6 +50,9 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_dedisperse_hd": ([_p, _int, _i64, _i64, _p, _p, _i64, _i64, _p], _int),
     "spp_fold": ([_p, _int, _i64, _i64, _p, _i32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                   _i64, _i32, _i32, _i32, _i64, _p, _p, _p, _i64, _p], _int),
+    "spp_fold_exact": ([_p, _i64, _i64, _p, _i32, ctypes.c_float, ctypes.c_float,
+                        ctypes.c_float, _i64, _i32, _i32, _i32, _i64, _p, _p, _p, _i64, _p],
+                       _int),
     "spp_dedisperse_noalloc_max_bytes": ([], _i64),
     "spp_dedisperse_noalloc": ([_p, _int, _int, _i64, _i64, _p, _i32, _i32, _p, _i64, _i64, _int,
                                 _p], _int),

@@ -6,9 +6,10 @@
 // subintegration with the reference's float64 arithmetic -- same operations in
 // the same order, each rounded (no fused multiply-adds), Python's float floor
 // division -- sums the subband's channels and adds the sum and the channel
-// count into the cell with one atomic each.  For 8-bit data the per-subband
-// sums are integers and every cell stays an integer below 2^24, so the float32
-// cells equal the reference's sequential float32 adds exactly, in any order.
+// count into the cell with one atomic each.  Float32 cells (spp_fold) are
+// order-dependent in their last bits for float32 data, and for 8-bit data once
+// a cell passes 2^24; the 8-bit form with 64-bit integer cells
+// (spp_fold_exact) is exact and deterministic for any length.
 #include <cmath>
 
 #include "spp_common.cuh"
@@ -36,6 +37,7 @@ struct FoldArgs {
   int64_t index;
   int32_t nbins, nsubs;
   float* fold_ar;
+  unsigned long long* fold_u64;  // 8-bit exact cells (spp_fold_exact), else null
   int32_t* count_ar;
   int64_t cells;  // nints * nsubs * nbins
 };
@@ -59,6 +61,18 @@ __global__ void k_fold(const FoldArgs a) {
   if (c1 <= c0) return;
   // row of channel c: isamp + delay, a negative one wrapping to the block's end
   // (numba's negative index); rows outside the block are never read
+  if (a.fold_u64) {  // 8-bit data, exact integer cells
+    const uint8_t* x = static_cast<const uint8_t*>(a.in);
+    unsigned long long s = 0;
+    for (int c = c0; c < c1; ++c) {
+      int64_t row = isamp + a.delays[c];
+      if (row < 0) row += a.nsamps;
+      if (row >= 0 && row < a.nsamps) s += x[a.nchans * row + c];
+    }
+    atomicAdd(a.fold_u64 + pos2, s);
+    atomicAdd(a.count_ar + pos2, c1 - c0);
+    return;
+  }
   float sum;
   if (a.is_f32) {
     const float* x = static_cast<const float*>(a.in);
@@ -87,12 +101,13 @@ __global__ void k_fold(const FoldArgs a) {
 
 using namespace spp;
 
-extern "C" int spp_fold(const void* in, int nbits, int64_t nchans, int64_t nsamps,
-                        const int32_t* delays, int32_t maxdelay, float tsamp, float period,
-                        float accel, int64_t total_nsamps, int32_t nbins, int32_t nints,
-                        int32_t nsubs, int64_t index, const int32_t* band_start, float* fold_ar,
-                        int32_t* count_ar, int64_t cells, void* stream) {
-  if (!in || !delays || !band_start || !fold_ar || !count_ar)
+static int fold_impl(const void* in, int nbits, int64_t nchans, int64_t nsamps,
+                     const int32_t* delays, int32_t maxdelay, float tsamp, float period,
+                     float accel, int64_t total_nsamps, int32_t nbins, int32_t nints,
+                     int32_t nsubs, int64_t index, const int32_t* band_start, float* fold_ar,
+                     unsigned long long* fold_u64, int32_t* count_ar, int64_t cells,
+                     void* stream) {
+  if (!in || !delays || !band_start || (!fold_ar && !fold_u64) || !count_ar)
     return fail(SPP_ERR_ARG, "spp_fold: null pointer");
   if (nbits != 8 && nbits != 32)
     return fail(SPP_ERR_UNSUPPORTED, "spp_fold takes 8-bit or float32 samples (unpack first)");
@@ -123,6 +138,7 @@ extern "C" int spp_fold(const void* in, int nbits, int64_t nchans, int64_t nsamp
   a.nbins = nbins;
   a.nsubs = nsubs;
   a.fold_ar = fold_ar;
+  a.fold_u64 = fold_u64;
   a.count_ar = count_ar;
   a.cells = cells;
   constexpr int kThreads = 256;
@@ -130,4 +146,25 @@ extern "C" int spp_fold(const void* in, int nbits, int64_t nchans, int64_t nsamp
   if (gx > INT32_MAX) return fail(SPP_ERR_SIZE, "spp_fold: block too long");
   k_fold<<<dim3((unsigned)gx, (unsigned)nsubs), kThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(a);
   return cuda_status(cudaGetLastError(), "fold launch");
+}
+
+extern "C" int spp_fold(const void* in, int nbits, int64_t nchans, int64_t nsamps,
+                        const int32_t* delays, int32_t maxdelay, float tsamp, float period,
+                        float accel, int64_t total_nsamps, int32_t nbins, int32_t nints,
+                        int32_t nsubs, int64_t index, const int32_t* band_start, float* fold_ar,
+                        int32_t* count_ar, int64_t cells, void* stream) {
+  return fold_impl(in, nbits, nchans, nsamps, delays, maxdelay, tsamp, period, accel,
+                   total_nsamps, nbins, nints, nsubs, index, band_start, fold_ar, nullptr,
+                   count_ar, cells, stream);
+}
+
+extern "C" int spp_fold_exact(const void* in, int64_t nchans, int64_t nsamps,
+                              const int32_t* delays, int32_t maxdelay, float tsamp, float period,
+                              float accel, int64_t total_nsamps, int32_t nbins, int32_t nints,
+                              int32_t nsubs, int64_t index, const int32_t* band_start,
+                              unsigned long long* fold_sums, int32_t* count_ar, int64_t cells,
+                              void* stream) {
+  return fold_impl(in, 8, nchans, nsamps, delays, maxdelay, tsamp, period, accel, total_nsamps,
+                   nbins, nints, nsubs, index, band_start, nullptr, fold_sums, count_ar, cells,
+                   stream);
 }

@@ -390,8 +390,14 @@ class Filterbank:
         """Fold into (subintegration, subband, phase bin) cells (base.py:1109-1207).
 
         The same checks, warnings, block plan and block index as the reference;
-        each block folds on the GPU (``spp_fold``; packed data is unpacked on the
-        device first) into device cells, divided by the counts at the end.
+        each block folds on the GPU (packed data is unpacked on the device
+        first) into device cells, divided by the counts at the end.  Integer
+        samples fold into exact 64-bit cells rounded to float32 once
+        (``spp_fold_exact``): identical to the reference's float32 cells while
+        a cell stays below 2^24, deterministic beyond.  Float32 samples fold
+        into float32 cells with atomic adds, so their last bits depend on the
+        order the adds land in (the reference adds sequentially): cubes agree
+        to float32 rounding and can differ from run to run in the last bits.
         """
         import warnings
 
@@ -411,7 +417,8 @@ class Filterbank:
         band_start = fold_band_start(h.nchans, nbands)
         dev = torch.device("cuda", torch.cuda.current_device())
         cells = nbins * nints * nbands
-        fold_ar = torch.zeros(cells, dtype=torch.float32, device=dev)
+        exact = h.nbits != 32  # integer samples: 64-bit integer cells, rounded once at the end
+        fold_ar = torch.zeros(cells, dtype=torch.int64 if exact else torch.float32, device=dev)
         count_ar = torch.zeros(cells, dtype=torch.int32, device=dev)
         ddev = torch.from_numpy(chan_delays).to(dev)
         bdev = torch.from_numpy(band_start).to(dev)
@@ -424,11 +431,18 @@ class Filterbank:
             else:
                 x, nb = raw, h.nbits
             # the reference indexes each block by ii * (gulp - max_delay) (base.py:1202)
-            _lib.check(lib.spp_fold(x.data_ptr(), nb, h.nchans, nsamps_r, ddev.data_ptr(),
-                                    max_delay, h.tsamp, period, accel, h.nsamples, nbins, nints,
-                                    nbands, ii * (gulp - max_delay), bdev.data_ptr(),
-                                    fold_ar.data_ptr(), count_ar.data_ptr(), cells, st))
-        f = fold_ar.cpu().numpy()
+            if exact:
+                _lib.check(lib.spp_fold_exact(x.data_ptr(), h.nchans, nsamps_r, ddev.data_ptr(),
+                                              max_delay, h.tsamp, period, accel, h.nsamples,
+                                              nbins, nints, nbands, ii * (gulp - max_delay),
+                                              bdev.data_ptr(), fold_ar.data_ptr(),
+                                              count_ar.data_ptr(), cells, st))
+            else:
+                _lib.check(lib.spp_fold(x.data_ptr(), nb, h.nchans, nsamps_r, ddev.data_ptr(),
+                                        max_delay, h.tsamp, period, accel, h.nsamples, nbins,
+                                        nints, nbands, ii * (gulp - max_delay), bdev.data_ptr(),
+                                        fold_ar.data_ptr(), count_ar.data_ptr(), cells, st))
+        f = fold_ar.cpu().numpy().astype(np.float32)
         c = count_ar.cpu().numpy()
         with np.errstate(divide="ignore", invalid="ignore"):
             f /= c

@@ -66,3 +66,32 @@ def test_fold_rejects_too_many_cells(torch_cuda):
     fb = _fb(np.zeros(1000 * 16, np.uint8), case, 8)
     with pytest.raises(ValueError):
         fb.fold(0.05, 1.0, nbins=50, nints=32, nbands=16)
+
+
+def test_fold_8bit_cells_past_2e24_exact_and_deterministic(torch_cuda):
+    """Cells whose totals pass 2^24 (constant 255 samples, one band, four bins:
+    ~4e5 adds of 255 per cell) stay exact: the cube is 255 to float32 rounding
+    and two runs agree bit for bit."""
+    case = {"nchans": 64, "fch1": 1400.0, "foff": -1.0, "tsamp": 1e-3, "nsamples": 1 << 15}
+    fb = _fb(np.full((1 << 15) * 64, 255, np.uint8), case, 8)
+    a = fb.fold(0.0173, 5.0, nbins=4, nints=1, nbands=1, gulp=4096)
+    b = fb.fold(0.0173, 5.0, nbins=4, nints=1, nbands=1, gulp=4096)
+    np.testing.assert_array_equal(a.data, b.data)
+    np.testing.assert_allclose(a.data, 255.0, rtol=2.0**-23)
+
+
+def test_fold_float32_long_block(torch_cuda, orc):
+    """Float32 cells fold with atomic adds in arrival order; against the
+    oracle's sequential float32 cells the means agree within the rounding of
+    the adds (relative 2^-24 per add into a cell, positive samples)."""
+    rng = np.random.default_rng(77)
+    n, nch = 60000, 32
+    case = {"nchans": nch, "fch1": 1400.0, "foff": -2.0, "tsamp": 5e-4, "nsamples": n}
+    vals = rng.normal(5.0, 1.0, n * nch).astype(np.float32)
+    fb = _fb(vals, case, 32)
+    fd = fb.fold(0.0311, 20.0, nbins=16, nints=4, nbands=4, gulp=8000)
+    d = np.atleast_1d(fb.header.get_dmdelays(20.0)).astype(np.int32)
+    sums, counts, cube = orc.filterbank_fold(vals, n, nch, d, 5e-4, 0.0311, 0.0, 16, 4, 4, 8000)
+    adds = counts / (nch // 4)  # one atomic add per (sample, band) into a cell
+    np.testing.assert_array_less(np.abs(fd.data - cube).ravel(),
+                                 (2.0 * adds * 2.0**-24 * np.abs(cube)).ravel() + 1e-30)
