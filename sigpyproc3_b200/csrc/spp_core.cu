@@ -113,7 +113,7 @@ static const std::vector<Variant>& variants() {
       mkb<2, 2, 8, 1, 2, 32, 80, 4>(), mkb<2, 2, 8, 1, 2, 32, 80>(), mkb<2, 2, 8, 1, 3, 32, 80>(),
       mkb<2, 2, 8, 1, 2, 32, 96>(), mkb<2, 2, 8, 1, 2, 32, 128>(),
       mkb<2, 2, 8, 1, 2, 64, 80>(), mkb<2, 2, 8, 1, 2, 64, 96>(),
-      mkb<2, 3, 8, 1, 2, 32, 112, 3>(),
+      mkb<2, 3, 8, 1, 2, 32, 112, 3>(), mkb<2, 3, 8, 1, 2, 32, 112, 2>(),
       mkb<2, 2, 8, 1, 2>(), mkb<2, 2, 8, 1, 3, 32>(), mkb<2, 2, 8, 1, 2, 32>(),
       mkb<2, 4, 8, 1, 2, 32>(), mkb<2, 2, 16, 1, 2, 32>(), mkb<2, 1, 8, 1, 3>(),
       mkb<1, 2, 8, 1, 2, 32, 80>(), mkb<1, 2, 8, 1, 2, 32, 128>(),

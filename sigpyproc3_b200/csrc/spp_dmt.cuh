@@ -888,6 +888,19 @@ __host__ __device__ constexpr int64_t bits_stage_bytes(int nb, int slab, int slo
   return (int64_t)slab * nb * slot_w * 4 + (int64_t)dw * slab * 8;
 }
 
+// Word layout of a thread's P words in the tile.  Odd P > 1: the P words are
+// consecutive (lane stride P words, coprime with the 32 banks: conflict-free),
+// so the P funnel shifts of a plane row need P + 1 shared loads; otherwise
+// they are interleaved across the warp (lane + 32 p), 2 loads per word.
+template <int P>
+struct BitsWords {
+  static constexpr bool kContig = (P & 1) && P > 1;
+  __host__ __device__ static constexpr int base(int tw, int lane) {
+    return kContig ? (tw * 32 + lane) * P : tw * 32 * P + lane;
+  }
+  __host__ __device__ static constexpr int pos(int p) { return kContig ? p : 32 * p; }
+};
+
 // One slab of SLAB channels through the carry-save network.  FULL: all
 // channels present (no predicates); otherwise channels >= nc add zeros.
 template <int NB, int P, int L, int SLAB, bool FULL, int SLOT = 0>
@@ -916,6 +929,7 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
         base[q] = sd + j * NB * slot_w + ow.x + wbase;
       }
       // one word position at a time: 4 channels x NB planes live, not x P
+      uint32_t carry[NB][4];  // consecutive words: the previous position's high word
 #pragma unroll
       for (int p = 0; p < P; ++p) {
         uint32_t x[NB][4];
@@ -925,8 +939,14 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
           for (int b = 0; b < NB; ++b) {
             uint32_t lo = 0u, hi = 0u;
             if (live[q]) {
-              lo = base[q][b * slot_w + 32 * p];
-              hi = base[q][b * slot_w + 32 * p + 1];
+              if constexpr (BitsWords<P>::kContig) {
+                lo = p == 0 ? base[q][b * slot_w] : carry[b][q];
+                hi = base[q][b * slot_w + p + 1];
+                carry[b][q] = hi;
+              } else {
+                lo = base[q][b * slot_w + 32 * p];
+                hi = base[q][b * slot_w + 32 * p + 1];
+              }
             }
             x[b][q] = __funnelshift_r(lo, hi, sh[q]);
           }
@@ -1063,10 +1083,10 @@ __device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
     return;
   }
 
-  // consumers: warp (dmw, tw); thread words w = tw*32*P + lane + 32*p
+  // consumers: warp (dmw, tw); thread words w = wbase + BitsWords<P>::pos(p)
   const int dmw = warp / TW, tw = warp % TW;
   const int dm = dm0 + dmw;
-  const int wbase = tw * 32 * P + lane;
+  const int wbase = BitsWords<P>::base(tw, lane);
   BitCounter<P, L> cnt;
   cnt.zero();
   bool ok = true;
@@ -1082,10 +1102,10 @@ __device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
     if (lane == 0) mbar_arrive(&empty[s]);
   }
   if (!ok || dm >= a.ndm) return;
-  // outputs: word p covers samples t0 + 32*(wbase + 32*p) + i
+  // outputs: word p covers samples t0 + 32*(wbase + pos(p)) + i
 #pragma unroll
   for (int p = 0; p < P; ++p) {
-    const int64_t tb = t0 + 32LL * (wbase + 32 * p);
+    const int64_t tb = t0 + 32LL * (wbase + BitsWords<P>::pos(p));
     if (a.out_kind == SPP_OUT_I32) {
       int32_t* out = static_cast<int32_t*>(a.out) + (int64_t)dm * a.out_stride + a.out_start;
       if (tb + 32 <= a.nvalid && ((reinterpret_cast<uintptr_t>(out + tb) & 15) == 0)) {
@@ -1319,7 +1339,7 @@ __device__ __forceinline__ void dmt_bits_wl_body(const WlArgs& w) {
   }
 
   const int dmw = warp / TW, tw = warp % TW;
-  const int wbase = tw * 32 * P + lane;
+  const int wbase = BitsWords<P>::base(tw, lane);
   BitCounter<P, L> cnt;
   cnt.zero();
   DmtItem it{};
@@ -1343,7 +1363,7 @@ __device__ __forceinline__ void dmt_bits_wl_body(const WlArgs& w) {
     if (k == nslab - 1 && dmw < it.nrows) {
 #pragma unroll
       for (int p = 0; p < P; ++p) {
-        const int64_t tb = it.t0 + 32LL * (wbase + 32 * p);
+        const int64_t tb = it.t0 + 32LL * (wbase + BitsWords<P>::pos(p));
         if (it.out_kind == SPP_OUT_I32) {
           int32_t* out = static_cast<int32_t*>(it.out) + (int64_t)dmw * it.out_stride + it.out_start;
 #pragma unroll
