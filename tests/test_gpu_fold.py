@@ -92,6 +92,6 @@ def test_fold_float32_long_block(torch_cuda, orc):
     fd = fb.fold(0.0311, 20.0, nbins=16, nints=4, nbands=4, gulp=8000)
     d = np.atleast_1d(fb.header.get_dmdelays(20.0)).astype(np.int32)
     sums, counts, cube = orc.filterbank_fold(vals, n, nch, d, 5e-4, 0.0311, 0.0, 16, 4, 4, 8000)
-    adds = counts / (nch // 4)  # one atomic add per (sample, band) into a cell
-    np.testing.assert_array_less(np.abs(fd.data - cube).ravel(),
-                                 (2.0 * adds * 2.0**-24 * np.abs(cube)).ravel() + 1e-30)
+    adds = counts.ravel() / (nch // 4)  # one atomic add per (sample, band) into a cell
+    got, ref = fd.data.ravel().astype(np.float64), cube.ravel().astype(np.float64)
+    np.testing.assert_array_less(np.abs(got - ref), 2.0 * adds * 2.0**-24 * np.abs(ref) + 1e-30)
