@@ -363,6 +363,31 @@ def main() -> None:
                      "tfactor": tf, "ffactor": ff, "seed": seed, "input_sha256": sha(vals)}
     meta["file_ops"] = fops
 
+    # ---- N3 PulseExtractor window arithmetic (readers.py:393-455): the
+    # reference's own property code, run on stand-in headers
+    names = {"t_decimate", "disp_delay", "block_delay", "nsamps", "nstart", "nstart_file",
+             "nsamps_file", "pulse_toa_block"}
+    pe_src = refload._extract(refload.SRC / "readers.py", names, class_name="PulseExtractor")
+    pe_ns: dict = {"np": np}
+    exec(compile("from __future__ import annotations\n" + pe_src, "readers.py", "exec"), pe_ns)
+    PE = type("PE", (), {n: property(pe_ns[n]) for n in names})
+    pe_cases = []
+    for toa, width, dm, toa_freq, nch_sub, nsamples in (
+            (3000, 8, 30.0, None, None, 6000), (40, 3, 10.0, 1480.0, 16, 6000),
+            (5990, 1, 50.0, None, 32, 6000), (100000, 64, 500.0, 1450.0, 40, 187520),
+            (12, 0, 2.0, None, None, 900), (700, 17, 120.0, 1500.5, 8, 4096)):
+        fch1, foff, tsamp, nch = 1510.0, -1.0, 320e-6, 64
+        f1 = toa_freq or fch1
+        nc = nch_sub or nch
+        sub = Hdr(nc, f1, foff)
+        e = PE()
+        e.pulse_toa, e.pulse_width, e.min_nsamps = toa, width, 64
+        e.sub_hdr = type("SH", (), {"nsamples": nsamples})()
+        e._disp_delay = int(max(np.abs(np.atleast_1d(cdd(sub.chan_freqs, dm, tsamp, f1))))) + width * 5
+        pe_cases.append({"args": [toa, width, dm, toa_freq, nch_sub, nsamples],
+                         "props": {n: int(getattr(e, n)) for n in sorted(names)}})
+    meta["pulse_extractor"] = pe_cases
+
     # ---- N1 real files: Filterbank.dedisperse over the reference's sigproc
     # test files -- its read_plan block loop (readers.py:171-233), its
     # unpack kernels as FileReader.creadinto applies them (io/fileio.py:284-292,

@@ -238,3 +238,21 @@ def test_sigproc_writer_roundtrip(tmp_path):
         w.cwrite(vals[320:])
     hdr = sigproc.read_header(tmp_path / "w.fil")
     assert hdr["nsamples"] == 40 and hdr["foff"] == -4.0 and hdr["nbits"] == 2
+
+
+def test_pulse_extractor_matches_reference_arithmetic(tmp_path, golden_meta):
+    """PulseExtractor's window (readers.py:393-455) against the reference's own
+    property code run on the same header values (tests/golden/make_golden.py)."""
+    from sigpyproc3_b200 import Header
+    from sigpyproc3_b200.readers import PulseExtractor
+
+    for case in golden_meta["pulse_extractor"]:
+        toa, width, dm, toa_freq, nch_sub, nsamples = case["args"]
+        h = Header(nchans=64, fch1=1510.0, foff=-1.0, tsamp=320e-6, nbits=8, nsamples=nsamples)
+        path = tmp_path / f"p{nsamples}.fil"
+        if not path.exists():
+            h.write_sigproc(path, np.zeros(nsamples * 64, np.uint8))
+        pe = PulseExtractor(str(path), toa, width, dm, min_nsamps=64, toa_freq=toa_freq,
+                            nchans=nch_sub)
+        got = {n: int(getattr(pe, n)) for n in case["props"]}
+        assert got == case["props"], (case["args"], got)
