@@ -11,7 +11,6 @@
 
 #include "spp_common.cuh"
 #include "spp_dmt.cuh"
-#include "spp_dmt_sub.cuh"
 
 namespace spp {
 
@@ -85,19 +84,12 @@ struct Variant {
   int single;  // 1: meant for one DM (time-split warps)
   int planes;  // 1: bit-sliced kernel over bit-plane rows (R = words per thread)
   int slot;    // > 0: kernel compiled for exactly this slot width (words)
-  int sub;     // 1: float64 kernel with shared channel-group sums (k_dmt_f64sub)
 };
-
-template <int R, int DW, int TW, int SLAB, int STAGES>
-static Variant mks() {
-  return Variant{32, SPP_ACC_F64, R, DW, TW, SLAB, STAGES, &k_dmt_f64sub<R, DW, TW, SLAB, STAGES>,
-                 0, 0, 0, 1};
-}
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
 static Variant mk(int single) {
   return Variant{NB, ACC, R, DW, TW, SLAB, STAGES, &k_dmt<NB, R, DW, TW, SLAB, STAGES, ACC>,
-                 single, 0, 0, 0};
+                 single, 0, 0};
 }
 
 // Bit-sliced counters hold sums below 2^kBitLevels.
@@ -107,7 +99,7 @@ template <int NB, int P, int DW, int TW, int STAGES, int SLAB = 64, int SLOT = 0
 static Variant mkb() {
   void (*fn)(const DmtArgs) = &k_dmt_bits<NB, P, DW, TW, STAGES, kBitLevels, SLAB, SLOT>;
   if constexpr (MINB > 0) fn = &k_dmt_bits_minb<NB, P, DW, TW, STAGES, kBitLevels, SLAB, SLOT, MINB>;
-  return Variant{NB, 0, P, DW, TW, SLAB, STAGES, fn, 0, 1, SLOT, 0};
+  return Variant{NB, 0, P, DW, TW, SLAB, STAGES, fn, 0, 1, SLOT};
 }
 
 #define SPP_INT_VARIANTS(NB)                    \
@@ -141,9 +133,6 @@ static const std::vector<Variant>& variants() {
       mk<32, 16, 4, 1, 16, 2, SPP_ACC_KAHAN32>(0),
       mk<32, 8, 2, 1, 16, 2, SPP_ACC_KAHAN32>(0),
       mk<32, 16, 2, 1, 16, 2, SPP_ACC_KAHAN32>(0),
-      // float32 input, fp64 accumulator, shared sums of four-channel groups
-      mks<16, 16, 1, 16, 2>(), mks<8, 16, 1, 16, 2>(), mks<16, 8, 1, 16, 2>(),
-      mks<8, 8, 2, 16, 2>(),
       // float32 input, fp64 accumulator (channel-ordered sums: the reference's)
       mk<32, 16, 4, 1, 16, 2, SPP_ACC_F64>(0),
       mk<32, 16, 2, 1, 16, 2, SPP_ACC_F64>(0),
@@ -171,9 +160,7 @@ static int slot_words(const Variant& v, int32_t span) {
   return need;
 }
 
-static int64_t smem_bytes(const Variant& v, int slot_w, int64_t sub_pbytes = 0) {
-  if (v.sub)
-    return v.STAGES * sub_stage_bytes(v.SLAB, slot_w, v.DW) + sub_pbytes + (2 * v.STAGES + 2) * 8;
+static int64_t smem_bytes(const Variant& v, int slot_w) {
   if (v.planes) return v.STAGES * bits_stage_bytes(v.nb, v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
   return v.STAGES * dmt_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
 }
@@ -253,7 +240,7 @@ static int launch_corner_turn(int nb, const void* in, int bitorder, int64_t ncha
 
 static int launch_dmt(const Variant& v, const DmtArgs& a, int64_t ntiles_t, int64_t ndm,
                       cudaStream_t st) {
-  const int64_t smem = smem_bytes(v, a.slot_w, a.sub_pbytes);
+  const int64_t smem = smem_bytes(v, a.slot_w);
   int rc = ensure_smem(v, smem);
   if (rc) return rc;
   dim3 grid((unsigned)ceil_div(ndm, v.DW), (unsigned)ntiles_t);
@@ -570,16 +557,7 @@ struct spp_dmt_plan {
   int32_t maxabs;
   std::vector<int> cands;      // candidate variant indices
   std::vector<int32_t> spans;  // span per candidate
-  std::vector<int64_t> pbytes; // per candidate: partial-row buffer bytes (group-sum kernels)
   int cur = 0;                 // index into cands
-  // group-sum kernels: pattern records per DM tile height
-  struct SubTable {
-    int dw = 0;
-    int32_t* d_tab = nullptr;
-    int64_t ngroups = 0;
-    std::vector<int64_t> npat_sum, bspan_sum;  // per (DM tile, 16-channel slab)
-  };
-  std::vector<SubTable> subs;
   // optional per-kernel timing: events (start, after corner turn, end) per execute
   bool timing = false;
   std::vector<cudaEvent_t> evpool;
@@ -596,85 +574,6 @@ static cudaEvent_t plan_event(spp_dmt_plan* p) {
 }
 
 static int plan_sign(const spp_dmt_plan* p) { return p->mode == SPP_MODE_ROLL ? -1 : 1; }
-
-// Pattern records of the group-sum kernels for DM tiles of `dw` trials: per
-// (tile, group of four channels) the distinct residual patterns of the
-// group's delays (relative to its first channel), each with the range of its
-// trials' first-channel delays, and per trial its pattern and shift; plus, per
-// (tile, slab of `slab` channels), the pattern count and the summed shift
-// ranges that size the partial-row buffer.
-static int build_sub_table(spp_dmt_plan* p, const int32_t* D, int dw, int slab,
-                           spp_dmt_plan::SubTable* out) {
-  const int64_t nchans = p->nchans, ndm = p->ndm;
-  const int64_t ngroups = nchans / kSubGroup;
-  const int64_t ntiles = ceil_div(ndm, dw);
-  const int64_t nslabs = ceil_div(nchans, slab);
-  const int rw = sub_rec_words(dw);
-  std::vector<int32_t> tab((size_t)(ntiles * ngroups * rw), 0);
-  out->npat_sum.assign((size_t)(ntiles * nslabs), 0);
-  out->bspan_sum.assign((size_t)(ntiles * nslabs), 0);
-  std::vector<int32_t> pr(3 * dw), bmin(dw), bmax(dw), base(dw);
-  std::vector<int> pat(dw);
-  for (int64_t t = 0; t < ntiles; ++t) {
-    for (int64_t g = 0; g < ngroups; ++g) {
-      int npat = 0;
-      for (int i = 0; i < dw; ++i) {
-        const int64_t ii = std::min<int64_t>(t * dw + i, ndm - 1);
-        const int32_t* row = D + ii * nchans + g * kSubGroup;
-        const int32_t b = row[0], r1 = row[1] - b, r2 = row[2] - b, r3 = row[3] - b;
-        int k = 0;
-        while (k < npat && !(pr[3 * k] == r1 && pr[3 * k + 1] == r2 && pr[3 * k + 2] == r3)) ++k;
-        if (k == npat) {
-          pr[3 * k] = r1; pr[3 * k + 1] = r2; pr[3 * k + 2] = r3;
-          bmin[k] = bmax[k] = b;
-          ++npat;
-        }
-        bmin[k] = std::min(bmin[k], b);
-        bmax[k] = std::max(bmax[k], b);
-        pat[i] = k;
-        base[i] = b;
-      }
-      int32_t* rec = tab.data() + (t * ngroups + g) * rw;
-      rec[0] = npat;
-      for (int i = 0; i < dw; ++i) {
-        const int64_t off = (int64_t)base[i] - bmin[pat[i]];
-        if (off < 0 || off > 0xffff) return SPP_ERR_UNSUPPORTED;
-        rec[4 + i] = (pat[i] << 16) | (int32_t)off;
-      }
-      int64_t bs = 0;
-      for (int k = 0; k < npat; ++k) {
-        int32_t* pe = rec + 4 + dw + 5 * k;
-        pe[0] = pr[3 * k]; pe[1] = pr[3 * k + 1]; pe[2] = pr[3 * k + 2];
-        pe[3] = bmin[k];
-        pe[4] = bmax[k] - bmin[k];
-        bs += pe[4];
-      }
-      const int64_t si = t * nslabs + (g * kSubGroup) / slab;
-      out->npat_sum[si] += npat;
-      out->bspan_sum[si] += bs;
-    }
-  }
-  out->dw = dw;
-  out->ngroups = ngroups;
-  cudaError_t e = cudaMalloc(&out->d_tab, sizeof(int32_t) * tab.size());
-  if (e != cudaSuccess) return cuda_status(e, "pattern table cudaMalloc");
-  e = cudaMemcpy(out->d_tab, tab.data(), sizeof(int32_t) * tab.size(), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return cuda_status(e, "pattern table upload");
-  return SPP_OK;
-}
-
-static const spp_dmt_plan::SubTable* sub_table(const spp_dmt_plan* p, int dw) {
-  for (const auto& t : p->subs)
-    if (t.dw == dw) return &t;
-  return nullptr;
-}
-
-// Partial-row buffer bytes of a group-sum variant: the largest slab's rows.
-static int64_t sub_pbytes(const spp_dmt_plan::SubTable& t, int64_t T) {
-  int64_t m = 0;
-  for (size_t i = 0; i < t.npat_sum.size(); ++i) m = std::max(m, t.npat_sum[i] * T + t.bspan_sum[i]);
-  return round_up(m * 8, 16);
-}
 
 static int64_t plan_nvalid(const spp_dmt_plan* p, int64_t nsamps) {
   return p->mode == SPP_MODE_ROLL ? nsamps : nsamps - p->maxabs;
@@ -741,39 +640,18 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
     span_of_dw.emplace_back(dw, span);
     return span;
   };
-  const bool sub_ok = nbits == 32 && acc == SPP_ACC_F64 && mode == SPP_MODE_DEDISPERSE &&
-                      ndm > 1 && nchans % kSubGroup == 0;
   for (int i = 0; i < (int)vs.size(); ++i) {
     const Variant& v = vs[i];
     if (v.nb != nbits || (nbits == 32 && v.acc != acc)) continue;
     if (ndm == 1 ? !v.single : v.single) continue;
     if (v.planes && nchans * ((1 << nbits) - 1) >= (1 << kBitLevels)) continue;
-    if (v.sub && !sub_ok) continue;
     const int32_t span = tile_span(v.DW);
     if (slot_words(v, span) < 0) continue;  // fixed slot too narrow for this table
-    int64_t pb = 0;
-    if (v.sub) {
-      if (!sub_table(p, v.DW)) {
-        spp_dmt_plan::SubTable t;
-        const int rc = build_sub_table(p, delays_host, v.DW, v.SLAB, &t);
-        if (rc == SPP_ERR_CUDA) {
-          if (t.d_tab) cudaFree(t.d_tab);
-          for (auto& u : p->subs) cudaFree(u.d_tab);
-          delete p;
-          return rc;
-        }
-        if (rc != SPP_OK) continue;
-        p->subs.push_back(std::move(t));
-      }
-      pb = sub_pbytes(*sub_table(p, v.DW), tile_T(v));
-    }
-    if (smem_bytes(v, slot_words(v, span), pb) > kMaxSmem) continue;
+    if (smem_bytes(v, slot_words(v, span)) > kMaxSmem) continue;
     p->cands.push_back(i);
     p->spans.push_back(span);
-    p->pbytes.push_back(pb);
   }
   if (p->cands.empty()) {
-    for (auto& u : p->subs) cudaFree(u.d_tab);
     delete p;
     return fail(SPP_ERR_UNSUPPORTED, "no kernel variant fits this delay table");
   }
@@ -790,8 +668,6 @@ int spp_dmt_plan_destroy(spp_dmt_plan* p) {
   if (!p) return SPP_OK;
   int rc = SPP_OK;
   for (cudaEvent_t e : p->evpool) cudaEventDestroy(e);
-  for (auto& t : p->subs)
-    if (t.d_tab) cudaFree(t.d_tab);
   if (p->d_delays) rc = cuda_status(cudaFree(p->d_delays), "plan cudaFree");
   delete p;
   return rc;
@@ -817,7 +693,7 @@ int spp_dmt_plan_describe(const spp_dmt_plan* p, int32_t* cfg) {
   const int slot = slot_words(v, p->spans[p->cur]);
   cfg[0] = v.nb; cfg[1] = v.R; cfg[2] = v.DW; cfg[3] = v.TW; cfg[4] = v.SLAB; cfg[5] = v.STAGES;
   cfg[6] = (int32_t)tile_T(v);
-  cfg[7] = (int32_t)smem_bytes(v, slot, p->pbytes[p->cur]);
+  cfg[7] = (int32_t)smem_bytes(v, slot);
   return SPP_OK;
 }
 
@@ -894,13 +770,6 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
   a.out_start = out_start;
   a.nvalid = g.nvalid;
   a.status = reinterpret_cast<uint32_t*>(ws);
-  if (v.sub) {
-    const spp_dmt_plan::SubTable* t = sub_table(p, v.DW);
-    if (!t) return fail(SPP_ERR_UNSUPPORTED, "pattern table missing");
-    a.sub_tab = t->d_tab;
-    a.sub_ngroups = t->ngroups;
-    a.sub_pbytes = (int32_t)p->pbytes[p->cur];
-  }
   rc = launch_dmt(v, a, g.ntiles_t, p->ndm, st);
   if (rc) return rc;
   if (p->timing) cudaEventRecord(ev[2], st);

@@ -284,10 +284,6 @@ struct DmtArgs {
   int64_t out_start;
   int64_t nvalid;
   uint32_t* status;
-  // shared channel-group sums (k_dmt_f64sub only)
-  const int32_t* sub_tab;  // records, (DM tile x group) x sub_rec_words(DW) int32
-  int64_t sub_ngroups;     // groups of four channels
-  int32_t sub_pbytes;      // bytes of the partial-row buffer
 };
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES>
