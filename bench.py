@@ -388,6 +388,14 @@ def run_gpu(args, rank, world, local):
             "served_over_plain": c3["served_over_plain"], "beams": 64,
             "ms_per_step": c3["ms_per_step"], "steps": c3["steps"]}
         torch.cuda.empty_cache()
+        c4 = workloads.measure_c4(args.chunks, args.budget_gb, local, 1)
+        secondary["config4"] = {
+            "metric": c4["metric"], "value": c4["value"], "unit": UNIT,
+            "latency_ms": c4["latency_ms"], "plain_per_call": c4["plain_per_call"]["value"],
+            "plain_latency_ms": c4["plain_per_call"]["latency_ms"],
+            "served_over_plain": c4["served_over_plain"], "chunks": args.chunks,
+            "batches": c4["batches"], "makespan_ms": c4["ms_per_step"]}
+        torch.cuda.empty_cache()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -298,9 +298,16 @@ def measure_c3(steps: int, warmup: int, beams: int, batch: int, rank: int, world
 
 def run_c4(args, rank, world, local, emit) -> None:
     """Config 4: served streaming search over 32 beams vs the plain per-call path."""
+    m = measure_c4(args.chunks, args.budget_gb, local, world)
+    if rank == 0:
+        emit(**m)
+
+
+def measure_c4(nchunks: int, budget_gb: float, local: int = 0, world: int = 1) -> dict:
+    """Config-4 measurements as the fields of one bench line (see run_c4)."""
     from .serve import BeamState, Chunk, Server, chunk_sizes, make_beams, plain_process
 
-    nbeams, nchunks = 32, args.chunks
+    nbeams = 32
     specs = make_beams(nbeams, seed=4)
     sizes = chunk_sizes(nchunks, seed=4)
     beam_of = np.arange(nchunks) % nbeams
@@ -339,11 +346,10 @@ def run_c4(args, rank, world, local, emit) -> None:
     rng = np.random.default_rng(40)
     arrivals = np.cumsum(rng.exponential(1.0 / (4.0 * plain_rate), size=nchunks))
     arrivals -= arrivals[0]
-    srv = Server(specs, hbm_budget=int(args.budget_gb * (1 << 30)), max_inflight=2,
+    srv = Server(specs, hbm_budget=int(budget_gb * (1 << 30)), max_inflight=2,
                  device=local)
     stats = srv.run_arrivals(mk_chunks(), arrivals)
-    if rank == 0:
-        emit(metric="DM-trial x samples/s, config 4 (served streaming search, continuous batching)",
+    return dict(metric="DM-trial x samples/s, config 4 (served streaming search, continuous batching)",
              value=stats["throughput"], unit=UNIT, n_gpus=world, steps=1, warmup=0,
              ms_per_step=stats["makespan_s"] * 1e3, higher_is_better=True, scaling="weak",
              vs_baseline=None, dtype="u1/u2/u4/u8->int32 (+f32 S/N)",
@@ -351,7 +357,7 @@ def run_c4(args, rank, world, local, emit) -> None:
              config={"workload": f"config 4: {nbeams} beams, nchans in 256/1024/4096, nbits "
                      f"1/2/4/8, {nchunks} chunks of 2^14..2^18 samples with carried overlap, "
                      "DM max U[500,3000] with 256-2048 trials, Poisson arrivals at 4x the plain "
-                     "capacity", "hbm_budget_gb": args.budget_gb},
+                     "capacity", "hbm_budget_gb": budget_gb},
              latency_ms={"p50": stats["p50_ms"], "p99": stats["p99_ms"]},
              batches=stats["batches"],
              plain_per_call={"value": plain_value, "unit": UNIT,
