@@ -314,6 +314,42 @@ int spp_boxcar_snr_robust(const void* in, int in_kind, int64_t nrows,
                           float* snr, int32_t* peak_index, void* workspace,
                           int64_t workspace_bytes, void* stream);
 
+/* ---- N3: matched filter -------------------------------------------------------
+ * MatchedFilter (core/filters.py:29-365) on the GPU.
+ * spp_row_loc_scale: per row of `nrows` (row stride `in_stride` elements, n
+ * samples, in_kind SPP_OUT_F32 / SPP_OUT_I32), the (loc, scale) pair of
+ * stats.estimate_zscore (core/stats.py:418-502) into loc_scale[row * 2 + 0/1]
+ * (device float64): method 0 = mean / population std, method 1 = median
+ * (float32, the two middle values averaged in float32) / IQR / 1.349 (exact
+ * order statistics); a scale within 1e-8 of 0 becomes 1.
+ * spp_zscore: out[i] = f32(f64(f32(in[i] - f32(loc))) / scale), the rounding
+ * of np.subtract(..., dtype=float32) then np.divide into float32.
+ * spp_matched_filter: kernels.convolve_templates (core/kernels.py:861-906)
+ * for the z-scored series z of n samples and FFT length nfft >= n
+ * (pocketfft's good size for real transforms, as the reference asks
+ * rocket_fft for): for template k (float64 samples temps[temp_offsets[k] ..
+ * temp_offsets[k+1]), reference bin ref_bins[k]) and t < n,
+ *   convs[k * n + t] = (sum_j h[j] z[((t + j - ref) mod nfft) mod n]
+ *                       - mu_k * sum_{m < nfft} z[m mod n]) / sigma_k
+ * with temp_stats[2k .. 2k+1] = (mu_k, sigma_k) = (sum h / nfft,
+ * sqrt(sum h^2 - (sum h)^2 / nfft)): the circular correlation with the
+ * template zero-padded to nfft, reference bin at 0, normalised to zero mean
+ * and unit power, that the reference computes by FFT; here direct, float64.
+ * The workspace (>= 16 B, device) receives sum z (float64) and, in its
+ * second 8 bytes, the first maximum of convs in (template, sample) order as
+ * an unsigned 64-bit key: high word the float's order-preserving bits, low
+ * word 0xFFFFFFFF - flat index. */
+int spp_row_loc_scale(const void* in, int in_kind, int64_t nrows, int64_t n,
+                      int64_t in_stride, int method, double* loc_scale,
+                      void* stream);
+int spp_zscore(const float* in, int64_t n, const double* loc_scale, float* out,
+               void* stream);
+int spp_matched_filter(const float* z, int64_t n, int64_t nfft,
+                       const double* temps, const int32_t* temp_offsets,
+                       const int32_t* ref_bins, const double* temp_stats,
+                       int ntemps, float* convs, void* workspace,
+                       int64_t workspace_bytes, void* stream);
+
 /* ---- R7: subband dedispersion ----------------------------------------------------
  * Stage 1 replaces kernels.subband (core/kernels.py:379-401) with a zeroed
  * output: out[t][s] = sum_{c: chan_to_sub[c]==s} x[t + delays[c]][c] for

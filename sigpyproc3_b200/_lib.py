@@ -83,6 +83,9 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_boxcar_snr": ([_p, _int, _i64, _i64, _i64, _p, _int, _p, _int, _p, _p, _p, _i64, _p],
                        _int),
     "spp_boxcar_filter": ([_p, _i64, _int, _p, _p], _int),
+    "spp_row_loc_scale": ([_p, _int, _i64, _i64, _i64, _int, _p, _p], _int),
+    "spp_zscore": ([_p, _i64, _p, _p, _p], _int),
+    "spp_matched_filter": ([_p, _i64, _i64, _p, _p, _p, _p, _int, _p, _p, _i64, _p], _int),
     "spp_boxcar_snr_robust_workspace_bytes": ([_i64, _i64, _int, _int], _i64),
     "spp_boxcar_snr_robust": ([_p, _int, _i64, _i64, _i64, _p, _int, _p, _int, _p, _p, _p, _i64,
                                _p], _int),

@@ -587,6 +587,142 @@ k_row_quantiles(const void* __restrict__ in, int kind, int64_t n, int64_t in_str
   }
 }
 
+// ---------------------------------------------------------------------------
+// MatchedFilter (core/filters.py:29-338, kernels.convolve_templates
+// core/kernels.py:861-906): the reference correlates the z-scored series with
+// each template by FFT over the series repeated to the FFT length N >= n
+// (circular_pad_goodsize), the template zero-padded to N, its reference bin
+// moved to index 0, time-reversed and normalised to zero mean and unit power
+// over all N entries.  That is, for t < n,
+//   conv[t] = (sum_j h[j] * z[((t + j - ref) mod N) mod n] - mu * S) / sigma,
+// mu = sum(h) / N, sigma = sqrt(sum(h^2) - sum(h)^2 / N), S = sum_{m<N} z[m mod n],
+// computed here directly in float64 (the templates are at most a few hundred
+// bins) and stored float32 as the reference's convs.
+// ---------------------------------------------------------------------------
+__global__ void k_zscore(const float* __restrict__ in, int64_t n, const double* __restrict__ ls,
+                         float* __restrict__ out) {
+  // np.subtract(x, loc, dtype=float32) then np.divide(., scale) into float32
+  const float loc = (float)ls[0];
+  const double scale = ls[1];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (float)((double)__fsub_rn(in[i], loc) / scale);
+}
+
+// mean and population standard deviation of one row in float64 (loc/scale
+// "mean"/"std"), one CTA per row
+__global__ void k_row_mean_std(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
+                               double* __restrict__ ls) {
+  __shared__ double red[32];
+  const char* base = static_cast<const char*>(in) + (int64_t)blockIdx.x * in_stride * 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += row_val(base, kind, i);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) red[warp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[w];
+    red[31] = t / (double)n;
+  }
+  __syncthreads();
+  const double mean = red[31];
+  __syncthreads();
+  double q = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double d = row_val(base, kind, i) - mean;
+    q += d * d;
+  }
+  for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+  if (lane == 0) red[warp] = q;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[w];
+    double sd = sqrt(t / (double)n);
+    if (fabs(sd) <= 1e-8) sd = 1.0;  // np.isclose(scale, 0) -> 1
+    ls[blockIdx.x * 2] = mean;
+    ls[blockIdx.x * 2 + 1] = sd;
+  }
+}
+
+// S = sum_{m < N} z[m mod n] in float64, one CTA
+__global__ void k_padded_sum(const float* __restrict__ z, int64_t n, int64_t nfft,
+                             double* __restrict__ out) {
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int64_t reps = nfft / n, rem = nfft % n;
+  double full = 0.0, part = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double v = (double)z[i];
+    full += v;
+    if (i < rem) part += v;
+  }
+  double t = full * (double)reps + part;
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if (lane == 0) red[warp] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double u = 0.0;
+    for (int w = 0; w < nw; ++w) u += red[w];
+    out[0] = u;
+  }
+}
+
+// First maximum of convs in flattened (template, sample) order, as np.argmax:
+// the float's order-preserving key in the high word and the complement of the
+// flat index in the low word, so atomicMax keeps the largest value and, among
+// equal values, the smallest index.
+__global__ void k_argmax_first(const float* __restrict__ v, int64_t count,
+                               unsigned long long* __restrict__ best) {
+  __shared__ unsigned long long red[32];
+  unsigned long long b = 0ull;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long key =
+        ((unsigned long long)f32_key(v[i]) << 32) | (unsigned long long)(0xFFFFFFFFu - (uint32_t)i);
+    if (key > b) b = key;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long ob = __shfl_xor_sync(0xffffffffu, b, o);
+    if (ob > b) b = ob;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w)
+      if (red[w] > b) b = red[w];
+    b = red[0] > b ? red[0] : b;
+    atomicMax(best, b);
+  }
+}
+
+// conv[k][t]: one thread per output sample of one template (blockIdx.y)
+__global__ void k_template_conv(const float* __restrict__ z, int64_t n, int64_t nfft,
+                                const double* __restrict__ temps, const int32_t* __restrict__ toff,
+                                const int32_t* __restrict__ tref, const double* __restrict__ tstat,
+                                const double* __restrict__ spad, float* __restrict__ convs) {
+  const int k = blockIdx.y;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const double* h = temps + toff[k];
+  const int len = toff[k + 1] - toff[k];
+  const int64_t ref = tref[k];
+  double acc = 0.0;
+  int64_t m = t - ref;  // padded index of h[0], taken mod N then mod n
+  m %= nfft;
+  if (m < 0) m += nfft;
+  for (int j = 0; j < len; ++j) {
+    acc += h[j] * (double)z[m % n];
+    if (++m == nfft) m = 0;
+  }
+  // tstat[k]: (mu, sigma) of the padded, normalised template
+  const double mu = tstat[2 * k], sigma = tstat[2 * k + 1];
+  convs[(int64_t)k * n + t] = (float)(sigma > 0.0 ? (acc - mu * spad[0]) / sigma : acc - mu * spad[0]);
+}
+
 template <typename F>
 static int dispatch_nb(int nbits, F&& f) {
   switch (nbits) {
@@ -833,6 +969,65 @@ int spp_boxcar_filter(const float* in, int64_t n, int width, float* out, void* s
   k_boxcar_filter<<<(unsigned)ceil_div(n, kBoxT), kBoxThreads, smem, as_stream(stream)>>>(
       in, n, width, pad_left, ref_bin, out);
   return cuda_status(cudaGetLastError(), "boxcar filter launch");
+}
+
+int spp_row_loc_scale(const void* in, int in_kind, int64_t nrows, int64_t n, int64_t in_stride,
+                      int method, double* loc_scale, void* stream) {
+  if (!in || !loc_scale) return fail(SPP_ERR_ARG, "spp_row_loc_scale: null pointer");
+  if (in_kind != SPP_OUT_F32 && in_kind != SPP_OUT_I32) return fail(SPP_ERR_ARG, "bad in_kind");
+  if (nrows <= 0 || nrows > 65535 || n <= 0) return fail(SPP_ERR_ARG, "bad sizes");
+  cudaStream_t st = as_stream(stream);
+  if (method == 0) {
+    k_row_mean_std<<<(unsigned)nrows, 256, 0, st>>>(in, in_kind, n, in_stride, loc_scale);
+    return cuda_status(cudaGetLastError(), "mean/std launch");
+  }
+  if (method != 1) return fail(SPP_ERR_ARG, "method must be 0 (mean/std) or 1 (median/iqr)");
+  SnrCfg cfg{};
+  cfg.nf = 1;
+  cfg.f[0] = 1;
+  const int64_t qsmem = (int64_t)kQRanks * kQBins * 4;
+  int rc = set_smem_attr(reinterpret_cast<const void*>(k_row_quantiles), qsmem);
+  if (rc) return rc;
+  k_row_quantiles<<<(unsigned)nrows, kQThreads, qsmem, st>>>(in, in_kind, n, in_stride, cfg,
+                                                             loc_scale);
+  return cuda_status(cudaGetLastError(), "row quantiles launch");
+}
+
+int spp_zscore(const float* in, int64_t n, const double* loc_scale, float* out, void* stream) {
+  if (!in || !loc_scale || !out) return fail(SPP_ERR_ARG, "spp_zscore: null pointer");
+  if (n <= 0) return fail(SPP_ERR_ARG, "empty series");
+  const unsigned blocks = (unsigned)std::min<int64_t>(ceil_div(n, 256), 148 * 16);
+  k_zscore<<<blocks, 256, 0, as_stream(stream)>>>(in, n, loc_scale, out);
+  return cuda_status(cudaGetLastError(), "zscore launch");
+}
+
+int spp_matched_filter(const float* z, int64_t n, int64_t nfft, const double* temps,
+                       const int32_t* temp_offsets, const int32_t* ref_bins,
+                       const double* temp_stats, int ntemps, float* convs, void* workspace,
+                       int64_t workspace_bytes, void* stream) {
+  if (!z || !temps || !temp_offsets || !ref_bins || !temp_stats || !convs || !workspace)
+    return fail(SPP_ERR_ARG, "spp_matched_filter: null pointer");
+  if (n <= 0 || nfft < n) return fail(SPP_ERR_ARG, "need 0 < n <= nfft");
+  if (ntemps <= 0 || ntemps > 65535) return fail(SPP_ERR_ARG, "bad template count");
+  if (workspace_bytes < 16) return fail(SPP_ERR_SIZE, "workspace < 16 B");
+  if ((int64_t)ntemps * n > 0xFFFFFFFFll) return fail(SPP_ERR_UNSUPPORTED, "ntemps * n >= 2^32");
+  cudaStream_t st = as_stream(stream);
+  double* spad = static_cast<double*>(workspace);
+  unsigned long long* best = reinterpret_cast<unsigned long long*>(spad + 1);
+  int rc = cuda_status(cudaMemsetAsync(best, 0, 8, st), "best clear");
+  if (rc) return rc;
+  k_padded_sum<<<1, 1024, 0, st>>>(z, n, nfft, spad);
+  rc = cuda_status(cudaGetLastError(), "padded sum launch");
+  if (rc) return rc;
+  dim3 grid((unsigned)ceil_div(n, 256), (unsigned)ntemps);
+  k_template_conv<<<grid, 256, 0, st>>>(z, n, nfft, temps, temp_offsets, ref_bins, temp_stats,
+                                        spad, convs);
+  rc = cuda_status(cudaGetLastError(), "template convolution launch");
+  if (rc) return rc;
+  const int64_t count = (int64_t)ntemps * n;
+  k_argmax_first<<<(unsigned)std::min<int64_t>(ceil_div(count, 256), 148 * 8), 256, 0, st>>>(
+      convs, count, best);
+  return cuda_status(cudaGetLastError(), "argmax launch");
 }
 
 int64_t spp_boxcar_snr_robust_workspace_bytes(int64_t nrows, int64_t n, int nfactors,

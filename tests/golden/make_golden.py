@@ -388,6 +388,33 @@ def main() -> None:
                          "props": {n: int(getattr(e, n)) for n in sorted(names)}})
     meta["pulse_extractor"] = pe_cases
 
+    # ---- N3 template bank: the reference's own Template.gen_* and
+    # MatchedFilter.get_box_width_spacing (core/filters.py:340-365, :508-579)
+    tsrc = refload._extract(refload.SRC / "core" / "filters.py",
+                            {"gen_boxcar", "gen_gaussian", "gen_lorentzian"}, class_name="Template")
+    wsrc = refload._extract(refload.SRC / "core" / "filters.py", {"get_box_width_spacing"},
+                            class_name="MatchedFilter")
+    t_ns: dict = {"np": np, "gaussian_fwhm_to_sigma": 1.0 / (2.0 * np.sqrt(2.0 * np.log(2.0))),
+                  "Template": object}
+    exec(compile("from __future__ import annotations\n" + tsrc + "\n" + wsrc, "filters.py",
+                 "exec"), t_ns)
+
+    def fake_cls(arr, width, ref_bin=0, ref="start", kind="custom"):
+        return arr, width, ref_bin, ref, kind
+
+    temps = []
+    for kind, widths in (("boxcar", t_ns["get_box_width_spacing"](32, 1.5)),
+                         ("gaussian", np.geomspace(1, 32, int(np.ceil(np.log(32) / np.log(1.5))) + 1)),
+                         ("lorentzian", np.geomspace(1, 32, int(np.ceil(np.log(32) / np.log(1.5))) + 1))):
+        for k, w in enumerate(widths):
+            arr, width, ref_bin, ref, kd = t_ns[f"gen_{kind}"](fake_cls, w)
+            out[f"temp_{kind}_{k}"] = np.asarray(arr)
+            temps.append({"kind": kind, "k": k, "width": float(width), "ref_bin": int(ref_bin),
+                          "ref": ref})
+    meta["templates"] = temps
+    meta["box_widths_32_1p5"] = [float(w) for w in t_ns["get_box_width_spacing"](32, 1.5)]
+    meta["box_widths_100_1p3"] = [float(w) for w in t_ns["get_box_width_spacing"](100, 1.3)]
+
     # ---- N1 real files: Filterbank.dedisperse over the reference's sigproc
     # test files -- its read_plan block loop (readers.py:171-233), its
     # unpack kernels as FileReader.creadinto applies them (io/fileio.py:284-292,

@@ -256,3 +256,39 @@ def test_pulse_extractor_matches_reference_arithmetic(tmp_path, golden_meta):
                             nchans=nch_sub)
         got = {n: int(getattr(pe, n)) for n in case["props"]}
         assert got == case["props"], (case["args"], got)
+
+
+def test_good_size_matches_pocketfft_rule():
+    """The FFT length the reference pads to (rocket_fft.good_size(n, real=True)):
+    pocketfft's rule, as scipy.fft.next_fast_len(n, real=True) applies it."""
+    from scipy import fft as sfft
+
+    from sigpyproc3_b200.filters import good_size_real
+
+    ns = list(range(1, 4000)) + [65535, 65536, 65537, 999983, 1 << 20, (1 << 21) - 1]
+    assert [good_size_real(n) for n in ns] == [sfft.next_fast_len(n, real=True) for n in ns]
+
+
+def test_template_bank_matches_reference(golden, golden_meta, orc):
+    """Template.gen_* and get_box_width_spacing against the reference's own code
+    (tests/golden/make_golden.py), for this package and for the oracle."""
+    from sigpyproc3_b200.filters import MatchedFilter, Template
+
+    np.testing.assert_array_equal(MatchedFilter.get_box_width_spacing(32, 1.5),
+                                  golden_meta["box_widths_32_1p5"])
+    np.testing.assert_array_equal(MatchedFilter.get_box_width_spacing(100, 1.3),
+                                  golden_meta["box_widths_100_1p3"])
+    by_kind = {}
+    for rec in golden_meta["templates"]:
+        t = getattr(Template, f"gen_{rec['kind']}")(rec["width"])
+        ref = golden[f"temp_{rec['kind']}_{rec['k']}"]
+        np.testing.assert_array_equal(t.data, ref)
+        assert t.data.dtype == ref.dtype
+        assert (t.ref_bin, t.ref) == (rec["ref_bin"], rec["ref"])
+        by_kind.setdefault(rec["kind"], []).append((ref, rec["ref_bin"]))
+    for kind, temps in by_kind.items():
+        _, bank = orc.template_bank(kind)
+        assert len(bank) == len(temps)
+        for (h, rb), (ref, rrb) in zip(bank, temps):
+            np.testing.assert_array_equal(np.asarray(h), ref)
+            assert rb == rrb
