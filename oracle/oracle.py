@@ -353,18 +353,20 @@ def zscore_f32(x: np.ndarray, loc_method: str, scale_method: str):
         loc = np.mean(x, dtype=np.float64)
     else:
         loc = np.float32(0.0)
+    # the scale is a float64 array in the reference (a strong type): the
+    # division runs in float64 and rounds into the float32 output
     if scale_method == "iqr":
         q = np.percentile(x.astype(np.float64), [25, 75])
-        scale = float((q[1] - q[0]) / 1.3489795003921634)
+        scale = np.float64((q[1] - q[0]) / 1.3489795003921634)
     elif scale_method == "std":
-        scale = float(np.std(x.astype(np.float64)))
+        scale = np.float64(np.std(x.astype(np.float64)))
     else:
-        scale = 1.0
+        scale = np.float32(1.0)
     if np.isclose(scale, 0):
-        scale = 1.0
+        scale = np.float64(1.0)
     z = np.subtract(x, loc, dtype=np.float32)
     np.divide(z, scale, out=z)
-    return z, loc, scale
+    return z, loc, float(scale)
 
 
 def template_bank(kind: str, nbins_max: int = 32, spacing_factor: float = 1.5):

@@ -60,9 +60,10 @@ class ZScoreResult:
     scale: np.ndarray
 
 
-@dataclass(frozen=True)
+@dataclass(frozen=True, eq=False)
 class Template:
-    """A pulse template (filters.py:366-587): samples, width, reference bin."""
+    """A pulse template (filters.py:366-587): samples, width, reference bin.
+    Templates compare by identity (their samples are arrays)."""
 
     data: np.ndarray
     width: float
