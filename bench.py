@@ -394,7 +394,8 @@ def run_gpu(args, rank, world, local):
             "latency_ms": c4["latency_ms"], "plain_per_call": c4["plain_per_call"]["value"],
             "plain_latency_ms": c4["plain_per_call"]["latency_ms"],
             "served_over_plain": c4["served_over_plain"], "chunks": args.chunks,
-            "batches": c4["batches"], "makespan_ms": c4["ms_per_step"]}
+            "batches": c4["batches"], "batch_chunks": c4["batch_chunks"],
+            "makespan_ms": c4["ms_per_step"]}
         torch.cuda.empty_cache()
     if rank == 0:
         line = {

@@ -114,6 +114,7 @@ class Server:
         self.streams = [torch.cuda.Stream(self.device) for _ in range(max_inflight)]
         self._rr = 0
         self.batches = 0
+        self.batch_sizes: list[int] = []
 
     # ---- sizing ----
     def _pick(self, st: BeamState) -> tuple[int, int]:
@@ -156,11 +157,17 @@ class Server:
         self.pending.append(c)
 
     def _admit(self) -> list[Chunk]:
+        """FIFO admission into one batch.  A batch holds at most
+        ``budget / max_inflight`` bytes (a single larger chunk goes alone), so
+        that when the queue is long the next batch still fits beside the
+        running one and its copies and corner turns overlap that batch's
+        transform instead of waiting for it to retire."""
         batch, used = [], 0
+        cap = self.budget // max(self.max_inflight, 1)
         while self.pending:
             c = self.pending[0]
             b = self.chunk_bytes(c)
-            if self.in_use + used + b > self.budget:
+            if self.in_use + used + b > self.budget or (batch and used + b > cap):
                 break
             # keep chunks of one beam in order: a beam's second chunk in the
             # same batch would need the first one's tail, which is fine since
@@ -250,6 +257,7 @@ class Server:
         self.inflight.append(_Batch(chunks, stream, ev, total, bufs, wls, status_host))
         self.in_use += total
         self.batches += 1
+        self.batch_sizes.append(len(chunks))
 
     def _retire(self, now_fn) -> int:
         n = 0
@@ -312,7 +320,7 @@ class Server:
         return {"throughput": units / makespan, "makespan_s": makespan,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3),
                 "p99_ms": float(np.percentile(lat, 99) * 1e3), "batches": self.batches,
-                "chunks": n}
+                "batch_chunks": list(self.batch_sizes), "chunks": n}
 
 
 def plain_process(beams: dict[int, BeamState] | None, chunk: Chunk, st: BeamState,

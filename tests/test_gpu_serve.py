@@ -114,6 +114,35 @@ def test_admission_respects_budget(torch_cuda):
     assert len(one.done) == 4
 
 
+def test_batch_cap_keeps_two_in_flight(torch_cuda):
+    """With the whole queue fitting the budget, a batch still takes at most
+    half of it (max_inflight=2), so the next batch can be admitted while the
+    first runs; a chunk larger than the cap goes alone."""
+    torch = torch_cuda
+    from sigpyproc3_b200.serve import Chunk, Server
+
+    specs = _beams()[:1]
+    data = _streams(specs, nchunks=6, seed=11)
+    lens, _, raws = data[0]
+    srv = Server(specs, hbm_budget=0, keep_dmt=False, max_inflight=2)
+    sizes = [srv.chunk_bytes(Chunk(0, k, int(lens[k]), None)) for k in range(6)]
+    srv.budget = sum(sizes) + 1
+    cap = srv.budget // 2
+    for k in range(6):
+        srv.submit(Chunk(0, k, int(lens[k]), torch.from_numpy(raws[k])))
+    seen = []
+    while srv.pending or srv.inflight:
+        before = srv.batches
+        srv.step()
+        if srv.batches > before:
+            b = srv.inflight[-1]
+            seen.append(len(b.chunks))
+            assert len(b.chunks) == 1 or b.bytes <= cap, (b.bytes, cap)
+        assert srv.in_use <= srv.budget
+    assert sum(seen) == 6 and len(seen) >= 2
+    assert srv.batch_sizes == seen
+
+
 def test_short_first_chunks(torch_cuda, orc):
     """Chunks shorter than the max delay: outputs start once the stream covers it."""
     torch = torch_cuda
