@@ -913,7 +913,10 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
   uint32_t cmid[NMID][P];
 #pragma unroll
   for (int m = 0; m < NMID; ++m) {  // 16 channels
-    uint32_t cq[4][P];
+    // the four quads' carries are folded pairwise as they arrive (quads 0+1
+    // into pa, quads 2+3 then pa into the per-16-channel carry), so at most
+    // two words per position are held
+    uint32_t pa[P], pw[P];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {    // 4 channels
       // per channel: staged row start and bit shift, decoded once
@@ -951,20 +954,26 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
             x[b][q] = __funnelshift_r(lo, hi, sh[q]);
           }
         }
+        uint32_t cq;
         if constexpr (NB == 2) {
           const uint32_t lo[4] = {x[0][0], x[0][1], x[0][2], x[0][3]};
           const uint32_t hi[4] = {x[NB - 1][0], x[NB - 1][1], x[NB - 1][2], x[NB - 1][3]};
-          cnt.quad2(p, lo, hi, cq[i][p]);  // weight 16
+          cnt.quad2(p, lo, hi, cq);  // weight 16
         } else {
           const uint32_t v[4] = {x[0][0], x[0][1], x[0][2], x[0][3]};
-          cnt.quad1(p, v, cq[i][p]);       // weight 4
+          cnt.quad1(p, v, cq);       // weight 4
+        }
+        constexpr int LQ = NB == 2 ? 4 : 2;  // level of the per-quad carries
+        if (i == 0 || i == 2) {
+          pw[p] = cq;
+        } else if (i == 1) {
+          csa(cnt.A[p][LQ], pw[p], cq, pa[p]);
+        } else {
+          uint32_t pb;
+          csa(cnt.A[p][LQ], pw[p], cq, pb);
+          csa(cnt.A[p][LQ + 1], pa[p], pb, cmid[m][p]);  // weight 64 (2-bit) / 16 (1-bit)
         }
       }
-    }
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-      const uint32_t w4[4] = {cq[0][p], cq[1][p], cq[2][p], cq[3][p]};
-      cnt.fold4(p, NB == 2 ? 4 : 2, w4, cmid[m][p]);  // weight 64 (2-bit) / 16 (1-bit)
     }
   }
   constexpr int LM = NB == 2 ? 6 : 4;  // level of the per-16-channel carries
