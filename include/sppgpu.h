@@ -188,8 +188,9 @@ int spp_dmt_plan_destroy(spp_dmt_plan* plan);
 /* valid output samples per row for an input of `nsamps` samples */
 int64_t spp_dmt_plan_nvalid(const spp_dmt_plan* plan, int64_t nsamps);
 int64_t spp_dmt_plan_workspace_bytes(const spp_dmt_plan* plan, int64_t nsamps);
-/* describe the chosen tiles: fills cfg[8] = {nbits, R, DW, TW, SLAB, STAGES,
- * T (samples per tile), smem bytes} */
+/* describe the chosen tiles: fills cfg[8] = {nbits | 256 * bit_sliced, R, DW,
+ * TW, SLAB, STAGES, T (samples per tile), smem bytes}; bit_sliced = 1 when the
+ * kernel counts over bit-plane rows (R = words per thread) */
 int spp_dmt_plan_describe(const spp_dmt_plan* plan, int32_t* cfg);
 /* override the tile shape (autotuner); variant index in [0, n) */
 int spp_dmt_plan_num_variants(const spp_dmt_plan* plan);

@@ -35,6 +35,15 @@ def variant_cfg(nbits: int, acc: int, variant: int) -> dict:
     return d
 
 
+def counter_fits(cfg: dict, nbits: int, nchans: int) -> bool:
+    """Whether a kernel variant can hold sums of ``nchans`` samples: the
+    bit-sliced kernels count below 2^14 (1-, 2-bit) or 2^16 (4-bit)."""
+    if not cfg["planes"]:
+        return True
+    levels = 16 if nbits == 4 else 14
+    return nchans * ((1 << nbits) - 1) < (1 << levels)
+
+
 def num_variants(nbits: int, acc: int = _lib.ACC_KAHAN32) -> int:
     return int(_lib.load().spp_wl_num_variants(nbits, acc))
 
@@ -89,6 +98,9 @@ class WorkList:
         out_ptr + r * out_stride * out_elem.  ``span``: the job's tile span
         (``tile_span`` of the signed delays for this variant's DW), when the
         caller has it cached."""
+        if not counter_fits(self.cfg, self.nbits, nchans):
+            raise ValueError(f"work-list variant {self.variant}: sums of {nchans} {self.nbits}-bit "
+                             "samples overflow its bit-sliced counter")
         dh = np.atleast_2d(delays_host).astype(np.int64) * sign
         ndm = dh.shape[0]
         if delays_dev.dtype != torch.int32 or delays_dev.stride(-1) != 1:

@@ -23,8 +23,9 @@ static WlVariant mkwl() {
 
 template <int NB, int P, int DW, int TW, int STAGES, int SLAB, int SLOT = 0, int MINB = 0>
 static WlVariant mkwlb() {
-  void (*fn)(const WlArgs) = &k_dmt_bits_wl<NB, P, DW, TW, STAGES, 14, SLAB, SLOT>;
-  if constexpr (MINB > 0) fn = &k_dmt_bits_wl_minb<NB, P, DW, TW, STAGES, 14, SLAB, SLOT, MINB>;
+  constexpr int L = BitsLevels<NB>::kLevels;
+  void (*fn)(const WlArgs) = &k_dmt_bits_wl<NB, P, DW, TW, STAGES, L, SLAB, SLOT>;
+  if constexpr (MINB > 0) fn = &k_dmt_bits_wl_minb<NB, P, DW, TW, STAGES, L, SLAB, SLOT, MINB>;
   return WlVariant{NB, 0, P, DW, TW, SLAB, STAGES, fn, 1, SLOT};
 }
 
@@ -39,6 +40,9 @@ static const std::vector<WlVariant>& wl_variants() {
       mkwlb<1, 2, 8, 1, 2, 64>(), mkwlb<1, 2, 8, 1, 3, 32>(),
       mkwlb<2, 2, 8, 1, 2, 32, 80, 4>(), mkwlb<2, 2, 8, 1, 2, 32, 128, 4>(),
       mkwlb<2, 2, 8, 1, 2, 64>(), mkwlb<2, 2, 8, 1, 3, 32>(),
+      // bit-sliced 4-bit ahead of the SIMD 4-bit kernels (faster at every span)
+      mkwlb<4, 2, 8, 1, 2, 16, 96, 3>(), mkwlb<4, 2, 8, 1, 2, 16, 128, 3>(),
+      mkwlb<4, 2, 8, 1, 2, 16>(),
       SPP_WL_INT(1), SPP_WL_INT(2), SPP_WL_INT(4), SPP_WL_INT(8), SPP_WL_INT(16),
       mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_KAHAN32>(), mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_KAHAN32>(),
       mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_F64>(),     mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_F64>(),
@@ -244,8 +248,10 @@ int spp_wl_corner_turn(int nbits, int acc, int variant, const void* in, int bito
   cudaStream_t st = stq(stream);
   if (nbits == 1)
     k_corner_turn_planes<1><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
-  else
+  else if (nbits == 2)
     k_corner_turn_planes<2><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
+  else
+    k_corner_turn_planes<4><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
   return cuda_status(cudaGetLastError(), "plane corner turn launch");
 }
 

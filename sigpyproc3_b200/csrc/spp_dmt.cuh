@@ -787,7 +787,7 @@ k_dmt_wl(const WlArgs w) {
 }
 
 // ----------------------------------------------------------------------------
-// Bit-sliced DM-time kernel for 1- and 2-bit data.
+// Bit-sliced DM-time kernel for 1-, 2- and 4-bit data.
 //
 // Planar "plane rows": row c*NB + k holds bit k of channel c's samples, 32
 // samples per word (LSB first).  A thread owns P words of time, interleaved
@@ -841,6 +841,28 @@ struct BitCounter {
     csa(A[p][2], fa, fb, ea);
     half(A[p][2], fc, eb);
     csa(A[p][3], ea, eb, out16);
+  }
+  // Four channels of 4-bit samples: x[b][q] is bit b (weight 2^b) of channel
+  // q.  Per level: the four input words of that weight plus the carries from
+  // the level below (2, 3, 4 and 4 of them).  Returns the weight-64 carry word.
+  __device__ __forceinline__ void quad4(int p, const uint32_t (&x)[4][4], uint32_t& out64) {
+    uint32_t c1a, c1b, c2a, c2b, c2c, c3a, c3b, c3c, c3d, c4a, c4b, c4c, c4d, c5a, c5b;
+    csa(A[p][0], x[0][0], x[0][1], c1a);
+    csa(A[p][0], x[0][2], x[0][3], c1b);
+    csa(A[p][1], x[1][0], x[1][1], c2a);
+    csa(A[p][1], x[1][2], x[1][3], c2b);
+    csa(A[p][1], c1a, c1b, c2c);
+    csa(A[p][2], x[2][0], x[2][1], c3a);
+    csa(A[p][2], x[2][2], x[2][3], c3b);
+    csa(A[p][2], c2a, c2b, c3c);
+    half(A[p][2], c2c, c3d);
+    csa(A[p][3], x[3][0], x[3][1], c4a);
+    csa(A[p][3], x[3][2], x[3][3], c4b);
+    csa(A[p][3], c3a, c3b, c4c);
+    csa(A[p][3], c3c, c3d, c4d);
+    csa(A[p][4], c4a, c4b, c5a);
+    csa(A[p][4], c4c, c4d, c5b);
+    csa(A[p][5], c5a, c5b, out64);
   }
   // Four channels of 1-bit samples.  Returns the weight-4 carry word.
   __device__ __forceinline__ void quad1(int p, const uint32_t (&x)[4], uint32_t& out4) {
@@ -901,6 +923,17 @@ struct BitsWords {
   __host__ __device__ static constexpr int pos(int p) { return kContig ? p : 32 * p; }
 };
 
+// Levels of the carry-save network per sample width: a quad of four channels
+// leaves one carry word of weight 2^kQuad (4 x (2^NB - 1) < 2^kQuad); the
+// counter needs kLevels levels for sums of 4096 channels (4096 x (2^NB - 1)
+// < 2^kLevels for 1-, 2- and 4-bit samples).
+template <int NB>
+struct BitsLevels {
+  static_assert(NB == 1 || NB == 2 || NB == 4, "bit-sliced kernels take 1-, 2- or 4-bit samples");
+  static constexpr int kQuad = NB == 4 ? 6 : NB == 2 ? 4 : 2;
+  static constexpr int kLevels = NB == 4 ? 16 : 14;
+};
+
 // One slab of SLAB channels through the carry-save network.  FULL: all
 // channels present (no predicates); otherwise channels >= nc add zeros.
 template <int NB, int P, int L, int SLAB, bool FULL, int SLOT = 0>
@@ -955,7 +988,9 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
           }
         }
         uint32_t cq;
-        if constexpr (NB == 2) {
+        if constexpr (NB == 4) {
+          cnt.quad4(p, x, cq);       // weight 64
+        } else if constexpr (NB == 2) {
           const uint32_t lo[4] = {x[0][0], x[0][1], x[0][2], x[0][3]};
           const uint32_t hi[4] = {x[NB - 1][0], x[NB - 1][1], x[NB - 1][2], x[NB - 1][3]};
           cnt.quad2(p, lo, hi, cq);  // weight 16
@@ -963,7 +998,7 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
           const uint32_t v[4] = {x[0][0], x[0][1], x[0][2], x[0][3]};
           cnt.quad1(p, v, cq);       // weight 4
         }
-        constexpr int LQ = NB == 2 ? 4 : 2;  // level of the per-quad carries
+        constexpr int LQ = BitsLevels<NB>::kQuad;  // level of the per-quad carries
         if (i == 0 || i == 2) {
           pw[p] = cq;
         } else if (i == 1) {
@@ -976,7 +1011,7 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
       }
     }
   }
-  constexpr int LM = NB == 2 ? 6 : 4;  // level of the per-16-channel carries
+  constexpr int LM = BitsLevels<NB>::kQuad + 2;  // level of the per-16-channel carries
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     if constexpr (NMID == 4) {
@@ -984,6 +1019,8 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
       uint32_t top;
       cnt.fold4(p, LM, w4, top);
       cnt.ripple(p, LM + 2, top);
+    } else if constexpr (NMID == 1) {
+      cnt.ripple(p, LM, cmid[0][p]);
     } else {
       uint32_t top;
       csa(cnt.A[p][LM], cmid[0][p], cmid[1][p], top);
@@ -998,7 +1035,7 @@ __device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
   constexpr int NWC = Sh::kNwc;
   constexpr int T = Sh::kT;
   constexpr int JJ = (SLAB + 31) / 32;
-  static_assert(SLAB == 32 || SLAB == 64, "slab of 32 or 64 channels");
+  static_assert(SLAB == 16 || SLAB == 32 || SLAB == 64, "slab of 16, 32 or 64 channels");
 
   extern __shared__ __align__(128) unsigned char smem[];
   uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);

@@ -182,7 +182,10 @@ class DMTPlan:
         cfg = (ctypes.c_int32 * 8)()
         _lib.check(_lib.load().spp_dmt_plan_describe(self._h, cfg))
         keys = ("nbits", "R", "DW", "TW", "SLAB", "STAGES", "T", "smem")
-        return dict(zip(keys, list(cfg)))
+        d = dict(zip(keys, list(cfg)))
+        d["bit_sliced"] = d["nbits"] >> 8
+        d["nbits"] &= 0xFF
+        return d
 
     @property
     def num_variants(self) -> int:

@@ -31,7 +31,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .batch import WorkList, corner_turn, planar_layout, tile_span, variant_cfg
+from .batch import WorkList, corner_turn, counter_fits, planar_layout, tile_span, variant_cfg
 from .header import Header
 from .search import boxcar_snr
 
@@ -127,7 +127,10 @@ class Server:
             cands = [self.variant] if self.variant is not None else \
                 range(lib.spp_wl_num_variants(st.nbits, acc))
             for v in cands:
-                dw = variant_cfg(st.nbits, acc, v)["DW"]
+                cfg = variant_cfg(st.nbits, acc, v)
+                if not counter_fits(cfg, st.nbits, st.nchans):
+                    continue
+                dw = cfg["DW"]
                 slot = int(lib.spp_wl_slot_words(st.nbits, acc, v, st.span(dw)))
                 if slot > 0 and lib.spp_wl_smem_bytes(st.nbits, acc, v, slot) <= 227 * 1024:
                     st.pick = (v, slot)

@@ -58,7 +58,8 @@ def _subset(kind):
     return d[np.linspace(0, 1023, 48).astype(int)]  # spread over the whole grid
 
 
-def _run_all_variants(torch, orc, vals, raw_host, nbits, order, d, nsamps, *, min_run=2):
+def _run_all_variants(torch, orc, vals, raw_host, nbits, order, d, nsamps, *, min_run=2,
+                      min_bit_sliced=0):
     from sigpyproc3_b200.dedisp import DMTPlan
 
     nvalid = nsamps - int(d.max())
@@ -66,7 +67,7 @@ def _run_all_variants(torch, orc, vals, raw_host, nbits, order, d, nsamps, *, mi
     rawd = torch.from_numpy(raw_host).cuda()
     plan = DMTPlan(d, NCHANS, nsamps, nbits=nbits, bitorder=order, out_dtype=torch.int32)
     out = torch.empty((d.shape[0], nvalid), dtype=torch.int32, device="cuda")
-    ran = 0
+    ran = sliced = 0
     for v in range(plan.num_variants):
         plan.set_variant(v)
         out.fill_(-1)
@@ -75,8 +76,9 @@ def _run_all_variants(torch, orc, vals, raw_host, nbits, order, d, nsamps, *, mi
         bad = np.argwhere(got != expect)
         assert bad.size == 0, (plan.describe(), bad[:5].tolist(), int(bad.shape[0]))
         ran += 1
+        sliced += plan.describe()["bit_sliced"]
     plan.close()
-    assert ran >= min_run
+    assert ran >= min_run and sliced >= min_bit_sliced, (ran, sliced)
     return expect
 
 
@@ -133,6 +135,9 @@ def test_c2_1bit(torch_cuda, orc, subset):
 
 
 def test_c2_4bit(torch_cuda, orc):
+    """4-bit samples near full scale: sums up to 15 x 4096 = 61 440 (the top
+    level of the 16-level bit-sliced counter) through the SIMD and the
+    bit-sliced kernels."""
     torch = torch_cuda
     d = _subset("top")
     nsamps = 8192 + int(d.max())
@@ -140,7 +145,8 @@ def test_c2_4bit(torch_cuda, orc):
     vals = rng.integers(0, 16, size=(nsamps, NCHANS), dtype=np.uint8)
     vals[1000:1000 + 34000] = 15
     vals = vals.ravel()
-    expect = _run_all_variants(torch, orc, vals, _pack(vals, 4, "big"), 4, "big", d, nsamps)
+    expect = _run_all_variants(torch, orc, vals, _pack(vals, 4, "big"), 4, "big", d, nsamps,
+                               min_bit_sliced=2)
     assert expect.max() == 15 * NCHANS
 
 
@@ -158,7 +164,7 @@ def test_c2_8bit_wide_sums(torch_cuda, orc):
     assert expect.max() == 255 * NCHANS
 
 
-@pytest.mark.parametrize("nbits", [1, 2])
+@pytest.mark.parametrize("nbits", [1, 2, 4])
 def test_c2_worklist_bit_sliced(torch_cuda, orc, nbits):
     """The persistent work-list kernels (served path) at 4096 channels."""
     torch = torch_cuda

@@ -292,3 +292,15 @@ def test_template_bank_matches_reference(golden, golden_meta, orc):
         for (h, rb), (ref, rrb) in zip(bank, temps):
             np.testing.assert_array_equal(np.asarray(h), ref)
             assert rb == rrb
+
+
+def test_counter_fits_bounds():
+    """Bit-sliced work-list kernels count below 2^14 (1-, 2-bit) or 2^16
+    (4-bit); SIMD kernels take any channel count."""
+    from sigpyproc3_b200.batch import counter_fits
+
+    sliced, simd = {"planes": 1}, {"planes": 0}
+    assert counter_fits(sliced, 4, 4369) and not counter_fits(sliced, 4, 4370)
+    assert counter_fits(sliced, 2, 5461) and not counter_fits(sliced, 2, 5462)
+    assert counter_fits(sliced, 1, 16383) and not counter_fits(sliced, 1, 16384)
+    assert counter_fits(simd, 4, 1 << 20)
