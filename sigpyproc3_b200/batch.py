@@ -37,10 +37,11 @@ def variant_cfg(nbits: int, acc: int, variant: int) -> dict:
 
 def counter_fits(cfg: dict, nbits: int, nchans: int) -> bool:
     """Whether a kernel variant can hold sums of ``nchans`` samples: the
-    bit-sliced kernels count below 2^14 (1-, 2-bit) or 2^16 (4-bit)."""
+    bit-sliced kernels count below 2^14 (1-, 2-bit), 2^16 (4-bit) or 2^20
+    (8-bit)."""
     if not cfg["planes"]:
         return True
-    levels = 16 if nbits == 4 else 14
+    levels = {4: 16, 8: 20}.get(nbits, 14)
     return nchans * ((1 << nbits) - 1) < (1 << levels)
 
 

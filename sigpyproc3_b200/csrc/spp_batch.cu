@@ -40,9 +40,11 @@ static const std::vector<WlVariant>& wl_variants() {
       mkwlb<1, 2, 8, 1, 2, 64>(), mkwlb<1, 2, 8, 1, 3, 32>(),
       mkwlb<2, 2, 8, 1, 2, 32, 80, 4>(), mkwlb<2, 2, 8, 1, 2, 32, 128, 4>(),
       mkwlb<2, 2, 8, 1, 2, 64>(), mkwlb<2, 2, 8, 1, 3, 32>(),
-      // bit-sliced 4-bit ahead of the SIMD 4-bit kernels (faster at every span)
+      // bit-sliced 4- and 8-bit ahead of the SIMD kernels (faster at every span)
       mkwlb<4, 2, 8, 1, 2, 16, 96, 3>(), mkwlb<4, 2, 8, 1, 2, 16, 128, 3>(),
       mkwlb<4, 2, 8, 1, 2, 16>(),
+      mkwlb<8, 2, 8, 1, 2, 16, 96, 2>(), mkwlb<8, 2, 8, 1, 2, 16, 0, 2>(),
+      mkwlb<8, 1, 8, 1, 2, 16>(),
       SPP_WL_INT(1), SPP_WL_INT(2), SPP_WL_INT(4), SPP_WL_INT(8), SPP_WL_INT(16),
       mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_KAHAN32>(), mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_KAHAN32>(),
       mkwl<32, 8, 8, 1, 32, 2, SPP_ACC_F64>(),     mkwl<32, 4, 8, 2, 32, 2, SPP_ACC_F64>(),
@@ -242,7 +244,8 @@ int spp_wl_corner_turn(int nbits, int acc, int variant, const void* in, int bito
   if (!v->planes) return spp_corner_turn(in, nbits, bitorder, nchans, nsamps, halo, planar, pitch_w, stream);
   if (!in || !planar || nchans <= 0 || nsamps <= 0 || (pitch_w & 3) || halo < 0 || (nchans * nbits) % 8)
     return fail(SPP_ERR_ARG, "bad corner-turn arguments");
-  dim3 grid((unsigned)ceil_div(nchans, kCtChans), (unsigned)std::min<int64_t>(ceil_div(pitch_w, kCtWords), 65535));
+  dim3 grid((unsigned)ceil_div(nchans, planes_ct_chans(nbits)),
+            (unsigned)std::min<int64_t>(ceil_div(pitch_w, kCtWords), 65535));
   const uint8_t* raw = static_cast<const uint8_t*>(in);
   uint32_t* pl = static_cast<uint32_t*>(planar);
   cudaStream_t st = stq(stream);
@@ -250,8 +253,10 @@ int spp_wl_corner_turn(int nbits, int acc, int variant, const void* in, int bito
     k_corner_turn_planes<1><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
   else if (nbits == 2)
     k_corner_turn_planes<2><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
-  else
+  else if (nbits == 4)
     k_corner_turn_planes<4><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
+  else
+    k_corner_turn_planes<8><<<grid, 256, 0, st>>>(raw, nchans, nsamps, bitorder, halo, pl, pitch_w);
   return cuda_status(cudaGetLastError(), "plane corner turn launch");
 }
 

@@ -67,6 +67,9 @@ __device__ __forceinline__ int64_t wrap_row(int64_t s, int64_t nsamps) {
 // ----------------------------------------------------------------------------
 constexpr int kCtChans = 64;
 constexpr int kCtWords = 16;
+// Channels per tile of the bit-plane corner turn: 8-bit data takes 32, so
+// the tile's raw bytes and its 8 plane rows per channel fit static shared memory.
+__host__ __device__ constexpr int planes_ct_chans(int nb) { return nb == 8 ? 32 : kCtChans; }
 
 template <int NB>
 __global__ void __launch_bounds__(256)
@@ -926,12 +929,46 @@ struct BitsWords {
 // Levels of the carry-save network per sample width: a quad of four channels
 // leaves one carry word of weight 2^kQuad (4 x (2^NB - 1) < 2^kQuad); the
 // counter needs kLevels levels for sums of 4096 channels (4096 x (2^NB - 1)
-// < 2^kLevels for 1-, 2- and 4-bit samples).
+// < 2^kLevels for 1-, 2-, 4- and 8-bit samples).
 template <int NB>
 struct BitsLevels {
-  static_assert(NB == 1 || NB == 2 || NB == 4, "bit-sliced kernels take 1-, 2- or 4-bit samples");
-  static constexpr int kQuad = NB == 4 ? 6 : NB == 2 ? 4 : 2;
-  static constexpr int kLevels = NB == 4 ? 16 : 14;
+  static_assert(NB == 1 || NB == 2 || NB == 4 || NB == 8, "bit-sliced kernels take 1-8 bit samples");
+  static constexpr int kQuad = NB == 8 ? 10 : NB == 4 ? 6 : NB == 2 ? 4 : 2;
+  static constexpr int kLevels = NB == 8 ? 20 : NB == 4 ? 16 : 14;
+};
+
+// Four channels of NB-bit samples through a carry-save network built level by
+// level: level B takes the four plane-B words (fetched through word(b, q),
+// aligned plane b of channel q, only when that level is reached, so few
+// input words are live) and the carries from level B - 1, adds them into
+// A[p][B] in pairs with carry-save adders (a half adder takes an odd one
+// out) and passes one carry per adder up.  Above the top plane the carries
+// are reduced the same way until one word is left: the carry of weight
+// 2^kQuad.  For NB = 2 this is quad2's network, adder for adder.
+template <int P, int L, int NB, int B, int NCIN>
+struct QuadLevel {
+  template <class F>
+  __device__ __forceinline__ static void run(BitCounter<P, L>& c, int p, F& word,
+                                             const uint32_t* cin, uint32_t& out) {
+    constexpr int NP = B < NB ? 4 : 0;
+    constexpr int NIN = NP + NCIN;
+    constexpr int NOUT = (NIN + 1) / 2;
+    uint32_t w[NIN];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) w[q] = word(B, q);
+#pragma unroll
+    for (int k = 0; k < NCIN; ++k) w[NP + k] = cin[k];
+    uint32_t co[NOUT];
+#pragma unroll
+    for (int k = 0; k < NIN / 2; ++k) csa(c.A[p][B], w[2 * k], w[2 * k + 1], co[k]);
+    if constexpr (NIN & 1) half(c.A[p][B], w[NIN - 1], co[NOUT - 1]);
+    if constexpr (NOUT == 1 && B + 1 >= NB) {
+      static_assert(B + 1 == BitsLevels<NB>::kQuad, "quad carry level");
+      out = co[0];
+    } else {
+      QuadLevel<P, L, NB, B + 1, NOUT>::run(c, p, word, co, out);
+    }
+  }
 };
 
 // One slab of SLAB channels through the carry-save network.  FULL: all
@@ -963,6 +1000,35 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
         const int2 ow = live[q] ? off[j] : make_int2(0, 0);  // (word, bit shift)
         sh[q] = ow.y;
         base[q] = sd + j * NB * slot_w + ow.x + wbase;
+      }
+      if constexpr (NB == 8) {
+        // eight planes: each plane word is loaded when its level of the
+        // network is reached (interleaved words: two loads per word)
+        static_assert(!BitsWords<P>::kContig, "8-bit bit-sliced kernels use interleaved words");
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          auto word = [&](int b, int q) -> uint32_t {
+            uint32_t lo = 0u, hi = 0u;
+            if (live[q]) {
+              lo = base[q][b * slot_w + 32 * p];
+              hi = base[q][b * slot_w + 32 * p + 1];
+            }
+            return __funnelshift_r(lo, hi, sh[q]);
+          };
+          uint32_t cq;
+          QuadLevel<P, L, NB, 0, 0>::run(cnt, p, word, nullptr, cq);  // weight 1024
+          constexpr int LQ = BitsLevels<NB>::kQuad;
+          if (i == 0 || i == 2) {
+            pw[p] = cq;
+          } else if (i == 1) {
+            csa(cnt.A[p][LQ], pw[p], cq, pa[p]);
+          } else {
+            uint32_t pb;
+            csa(cnt.A[p][LQ], pw[p], cq, pb);
+            csa(cnt.A[p][LQ + 1], pa[p], pb, cmid[m][p]);
+          }
+        }
+        continue;
       }
       // one word position at a time: 4 channels x NB planes live, not x P
       uint32_t carry[NB][4];  // consecutive words: the previous position's high word
@@ -1203,13 +1269,14 @@ __global__ void __launch_bounds__(256)
 k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t nsamps,
                      int bitorder, int64_t halo, uint32_t* __restrict__ planar,
                      int64_t pitch_w) {
+  constexpr int CC = planes_ct_chans(NB);
   constexpr int RT = kCtWords * 32;
-  constexpr int SB = kCtChans * NB / 8;
+  constexpr int SB = CC * NB / 8;
   constexpr int SBP = SB + 4;
   __shared__ __align__(16) uint8_t s_raw[RT * SBP];
-  __shared__ uint32_t s_out[kCtChans * NB][kCtWords + 1];
-  const int64_t c0 = (int64_t)blockIdx.x * kCtChans;
-  const int nc = (int)((nchans - c0) < kCtChans ? (nchans - c0) : kCtChans);
+  __shared__ uint32_t s_out[CC * NB][kCtWords + 1];
+  const int64_t c0 = (int64_t)blockIdx.x * CC;
+  const int nc = (int)((nchans - c0) < CC ? (nchans - c0) : CC);
   const int seg = (nc * NB + 7) / 8;
   const int64_t rowbytes = nchans * NB / 8;
   const int64_t segstart = c0 * NB / 8;
@@ -1235,8 +1302,8 @@ k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t ns
       }
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kCtChans * kCtWords; idx += blockDim.x) {
-      const int c = idx % kCtChans, w = idx / kCtChans;
+    for (int idx = threadIdx.x; idx < CC * kCtWords; idx += blockDim.x) {
+      const int c = idx % CC, w = idx / CC;
       uint32_t v[NB];
 #pragma unroll
       for (int b = 0; b < NB; ++b) v[b] = 0;
@@ -1253,7 +1320,7 @@ k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t ns
       for (int b = 0; b < NB; ++b) s_out[c * NB + b][w] = v[b];
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < kCtChans * NB * kCtWords; idx += blockDim.x) {
+    for (int idx = threadIdx.x; idx < CC * NB * kCtWords; idx += blockDim.x) {
       const int w = idx % kCtWords, rr = idx / kCtWords;
       if (rr < nc * NB && w0 + w < pitch_w) planar[(c0 * NB + rr) * pitch_w + w0 + w] = s_out[rr][w];
     }

@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .batch import WorkList, corner_turn, planar_layout, tile_span, variant_cfg
+from .batch import WorkList, planar_layout, tile_span, variant_cfg
 from .header import Header
 from .search import boxcar_snr
 
@@ -111,22 +111,27 @@ class SubbandSearch:
         self.wl2 = WorkList(16, self.v2, device=self.device)
         slot1 = self.wl1.slot_words(span1)
         slot2 = self.wl2.slot_words(span2)
+        if slot1 < 0 or slot2 < 0:
+            raise ValueError(f"work-list variants {variants}: a fixed slot is narrower than the "
+                             "plan's tile span")
         self.beams: list[BeamBuffers] = []
         for ns in nsamps_list:
             ns = int(ns)
             nv = p.nvalid(ns)
             if nv <= 0:
                 raise ValueError(f"beam of {ns} samples is shorter than the max delay {p.max_eff}")
-            halo1, pitch1 = planar_layout(8, self.cfg1["T"], ns, 0, p.max_rel, slot1)
+            # stage-1 planar rows as its kernel reads them (one row per
+            # channel, or eight bit-plane rows for a bit-sliced kernel)
+            halo1, pitch1, rpc1 = self.wl1.layout(ns, 0, p.max_rel, slot1)
             _, pitch2 = planar_layout(16, self.cfg2["T"], nv, 0, int(p.dsub.max()), slot2)
             pitch2 = max(pitch2, int(math.ceil(ns / 2)) + 4)
             pitch2 += (-pitch2) % 4
             raw = torch.empty(ns * p.nchans, dtype=torch.uint8, device=self.device)
-            planar = torch.empty(p.nchans * pitch1, dtype=torch.int32, device=self.device)
+            planar = torch.empty(p.nchans * rpc1 * pitch1, dtype=torch.int32, device=self.device)
             sub = torch.zeros(p.ngroups * p.nsub * pitch2, dtype=torch.int32, device=self.device)
             dmt = torch.empty((p.ndm, nv), dtype=torch.int32, device=self.device)
             b = BeamBuffers(raw, ns, planar, sub, dmt, nv)
-            b.halo1, b.pitch1, b.pitch2 = halo1, pitch1, pitch2
+            b.halo1, b.pitch1, b.pitch2, b.rpc1 = halo1, pitch1, pitch2, rpc1
             self.beams.append(b)
             self._add_jobs(b)
         self.wl1.finalize(span1)
@@ -138,7 +143,8 @@ class SubbandSearch:
         for s in range(p.nsub):
             c0 = s * p.cps
             self.wl1.add_job(
-                planar_ptr=b.planar.data_ptr() + c0 * b.pitch1 * 4, pitch_w=b.pitch1, halo=b.halo1,
+                planar_ptr=b.planar.data_ptr() + c0 * b.rpc1 * b.pitch1 * 4, pitch_w=b.pitch1,
+                halo=b.halo1,
                 nchans=p.cps, delays_dev=self.rel_dev[:, c0:], delays_host=p.rel[:, c0:c0 + p.cps],
                 out_ptr=b.sub.data_ptr() + s * b.pitch2 * 4, out_stride=p.nsub * b.pitch2 * 2,
                 out_start=0, out_elem=2, nvalid=b.nsamps, out_kind=_lib.OUT_U16)
@@ -155,8 +161,8 @@ class SubbandSearch:
         st = stream or torch.cuda.current_stream(self.device)
         p = self.plan
         for b in self.beams:
-            corner_turn(b.raw, 8, _lib.BITORDER_BIG, p.nchans, b.nsamps, b.halo1, b.planar,
-                        b.pitch1, stream=st)
+            self.wl1.corner_turn(b.raw, _lib.BITORDER_BIG, p.nchans, b.nsamps, b.halo1, b.planar,
+                                 b.pitch1, stream=st)
         self.wl1.launch(st)
         self.wl2.launch(st)
         if snr:

@@ -178,7 +178,7 @@ def run_c3(args, rank, world, local, emit) -> None:
     S/N peaks; each batch of beams is one CUDA graph of persistent launches.
     Also times the plain per-call path (one brute-force dedispersion + S/N per
     beam and DM) on a subset."""
-    m = measure_c3(steps, warmup, args.beams, args.batch, rank, world)
+    m = measure_c3(max(args.steps, 1), max(args.warmup, 1), args.beams, args.batch, rank, world)
     if rank == 0:
         emit(**m)
 
@@ -187,6 +187,7 @@ def measure_c3(steps: int, warmup: int, beams: int, batch: int, rank: int, world
     """Config-3 measurements as the fields of one bench line (see run_c3)."""
     from .dedisp import dedisperse_block
     from .search import boxcar_snr
+    from .batch import num_variants
     from .subband import SubbandPlan, SubbandSearch
 
     g = synth.C3
@@ -201,8 +202,13 @@ def measure_c3(steps: int, warmup: int, beams: int, batch: int, rank: int, world
     # autotune the two stages on the first batch
     tune_lens = lens[lo:lo + batch]
     best, best_ms = (0, 0), None
-    for v1, v2 in ((0, 0), (1, 0), (2, 0), (3, 0)):
-        srch = SubbandSearch(plan, tune_lens, factors=factors, widths=widths, variants=(v1, v2))
+    for v1 in range(num_variants(8)):  # stage 1: bit-sliced and SIMD 8-bit kernels
+        v2 = 0
+        try:
+            srch = SubbandSearch(plan, tune_lens, factors=factors, widths=widths,
+                                 variants=(v1, v2))
+        except ValueError:  # fixed slot too narrow for this plan
+            continue
         for b in srch.beams:
             synth.gauss_u8_device(b.raw.numel(), 99, 96.0, 12.0, out=b.raw)
         srch.run()

@@ -160,11 +160,11 @@ def test_c2_8bit_wide_sums(torch_cuda, orc):
     vals = rng.integers(200, 256, size=(nsamps, NCHANS), dtype=np.uint8)
     vals[1000:1000 + 34000] = 255
     vals = vals.ravel()
-    expect = _run_all_variants(torch, orc, vals, vals, 8, "big", d, nsamps)
+    expect = _run_all_variants(torch, orc, vals, vals, 8, "big", d, nsamps, min_bit_sliced=1)
     assert expect.max() == 255 * NCHANS
 
 
-@pytest.mark.parametrize("nbits", [1, 2, 4])
+@pytest.mark.parametrize("nbits", [1, 2, 4, 8])
 def test_c2_worklist_bit_sliced(torch_cuda, orc, nbits):
     """The persistent work-list kernels (served path) at 4096 channels."""
     torch = torch_cuda

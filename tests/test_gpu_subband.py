@@ -33,7 +33,14 @@ def test_subband_search_small(torch_cuda, orc):
     plan = SubbandPlan(h, dms, nsub=16, group=16)
     lens = [6000, 9000, 12000]
     factors, widths = (1, 2, 4), (1, 2, 4, 8, 16, 32, 64, 128, 256)
-    for v1, v2 in ((0, 0), (2, 1)):
+    from sigpyproc3_b200.batch import num_variants, variant_cfg
+    from sigpyproc3_b200 import _lib
+
+    # stage 1 through a bit-sliced kernel (eight plane rows per channel) and
+    # through a SIMD one
+    kinds = [variant_cfg(8, _lib.ACC_KAHAN32, v)["planes"] for v in range(num_variants(8))]
+    pairs = ((kinds.index(1), 0), (kinds.index(0), 1))
+    for v1, v2 in pairs:
         srch = SubbandSearch(plan, lens, factors=factors, widths=widths, variants=(v1, v2))
         data = [_beam(30 + i, n, 256) for i, n in enumerate(lens)]
         for b, x in zip(srch.beams, data):

@@ -303,4 +303,5 @@ def test_counter_fits_bounds():
     assert counter_fits(sliced, 4, 4369) and not counter_fits(sliced, 4, 4370)
     assert counter_fits(sliced, 2, 5461) and not counter_fits(sliced, 2, 5462)
     assert counter_fits(sliced, 1, 16383) and not counter_fits(sliced, 1, 16384)
+    assert counter_fits(sliced, 8, 4112) and not counter_fits(sliced, 8, 4113)
     assert counter_fits(simd, 4, 1 << 20)
