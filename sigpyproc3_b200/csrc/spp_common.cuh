@@ -26,6 +26,9 @@ static inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b
 //   [0] error bits (SPP_DEV_* below), [1] first failing block, [2] detail,
 //   [3] reserved.
 constexpr int64_t kStatusBytes = 256;  // keeps the data that follows 256-B aligned
+// Word of the status block where the float corner turn flags samples that
+// are not normal float32 (words 0-3 are the device status).
+constexpr int kSpecialWord = 16;
 enum : uint32_t {
   SPP_DEV_TIMEOUT = 1u,   // a bounded mbarrier wait expired
   SPP_DEV_RANGE = 2u,     // a delay fell outside the declared range (clamped)

@@ -217,7 +217,7 @@ static int ensure_smem(const Variant& v, int64_t bytes) {
 static int launch_corner_turn(int nb, const void* in, int bitorder, int64_t nchans,
                               int64_t nsamps, const Geometry& g, void* planar, cudaStream_t st,
                               const double* zdm = nullptr, const float* chanwts = nullptr,
-                              const float* bpass = nullptr) {
+                              const float* bpass = nullptr, uint32_t* special = nullptr) {
   if (g.planes) {
     dim3 grid((unsigned)ceil_div(nchans, planes_ct_chans(nb)),
               (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, kCtWords), 65535));
@@ -238,7 +238,7 @@ static int launch_corner_turn(int nb, const void* in, int bitorder, int64_t ncha
               (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, 32), 65535));
     k_corner_turn_f32<<<grid, 256, 0, st>>>(static_cast<const float*>(in), nchans, nsamps,
                                             g.halo, static_cast<float*>(planar), g.pitch_w,
-                                            zdm, chanwts, bpass);
+                                            zdm, chanwts, bpass, special);
   } else {
     dim3 grid((unsigned)ceil_div(nchans, kCtChans),
               (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, kCtWords), 65535));
@@ -764,8 +764,16 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
     rc = cuda_status(cudaGetLastError(), "zero-DM row sums");
     if (rc) return rc;
   }
+  // float64 sums of float32 rows: the corner turn flags samples that are not
+  // normal floats (word kSpecialWord of the status block, cleared here)
+  uint32_t* special = nullptr;
+  if (p->nbits == 32 && v.acc == SPP_ACC_F64) {
+    special = reinterpret_cast<uint32_t*>(ws) + kSpecialWord;
+    rc = cuda_status(cudaMemsetAsync(special, 0, 4, st), "special-value flag clear");
+    if (rc) return rc;
+  }
   rc = launch_corner_turn(p->nbits, in, p->bitorder, p->nchans, nsamps, g, planar, st, zd_rows,
-                          zd_chanwts, zd_bpass);
+                          zd_chanwts, zd_bpass, special);
   if (rc) return rc;
   if (p->timing) cudaEventRecord(ev[1], st);
   DmtArgs a{};
@@ -787,6 +795,7 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
   a.out_start = out_start;
   a.nvalid = g.nvalid;
   a.status = reinterpret_cast<uint32_t*>(ws);
+  a.special = special;
   rc = launch_dmt(v, a, g.ntiles_t, p->ndm, st);
   if (rc) return rc;
   if (p->timing) cudaEventRecord(ev[2], st);

@@ -136,19 +136,39 @@ k_corner_turn_int(const uint8_t* __restrict__ raw, int64_t nchans, int64_t nsamp
   }
 }
 
+// IEEE-754 binary32 -> binary64 for normal numbers by field arithmetic:
+// (-1)^s 2^(e-127) (1 + m 2^-23) is the binary64 number with the same sign,
+// biased exponent e - 127 + 1023 = e + 896 and significand m followed by 29
+// zero bits.  The high word is sign | (e + 896) << 20 | m >> 3, i.e.
+// ((|u| >> 3) + (896 << 20)) | sign, and the low word m << 29 = u << 29.
+// Integer-pipe work, so it runs beside the conversion unit's F2F; zero,
+// subnormals, infinities and NaN are not handled (the caller checks
+// f32_is_normal over its data first).
+__device__ __forceinline__ bool f32_is_normal(float x) {
+  return ((__float_as_uint(x) & 0x7fffffffu) - 0x00800000u) < 0x7f000000u;  // 1 <= e <= 254
+}
+__device__ __forceinline__ double f64_of_normal_f32(float x) {
+  const uint32_t u = __float_as_uint(x);
+  const uint32_t hi = (((u & 0x7fffffffu) >> 3) + (896u << 20)) | (u & 0x80000000u);
+  return __hiloint2double((int)hi, (int)(u << 29));
+}
+
 // Corner turn for float32 data, optionally fused with zero-DM subtraction
 // (kernels.remove_zerodm, core/kernels.py:465-505):
 //   y = f32((f64(x) - zdm[t] * f64(chanwts[c])) + f64(bpass[c]))
-// computed with round-to-nearest intrinsics (no contraction).
+// computed with round-to-nearest intrinsics (no contraction).  `special`
+// (optional): set to 1 when any sample taken from the block (after zero-DM)
+// is not a normal float32.
 static __global__ void __launch_bounds__(256)
 k_corner_turn_f32(const float* __restrict__ raw, int64_t nchans, int64_t nsamps,
                   int64_t halo, float* __restrict__ planar, int64_t pitch,
                   const double* __restrict__ zdm, const float* __restrict__ chanwts,
-                  const float* __restrict__ bpass) {
+                  const float* __restrict__ bpass, uint32_t* __restrict__ special = nullptr) {
   __shared__ float tile[32][33];
   const int64_t c0 = (int64_t)blockIdx.x * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
   const int64_t nty = (pitch + 31) / 32;
+  bool odd = false;  // a sample from the block that is not a normal float32
   for (int64_t by = blockIdx.y; by < nty; by += gridDim.y) {
     const int64_t p0 = by * 32;  // planar column (sample + halo)
     for (int i = ty; i < 32; i += 8) {
@@ -162,6 +182,7 @@ k_corner_turn_f32(const float* __restrict__ raw, int64_t nchans, int64_t nsamps,
           const double t2 = __dsub_rn((double)v, t1);
           v = (float)__dadd_rn(t2, (double)bpass[c]);
         }
+        odd |= !f32_is_normal(v);
       }
       tile[i][tx] = v;
     }
@@ -173,6 +194,8 @@ k_corner_turn_f32(const float* __restrict__ raw, int64_t nchans, int64_t nsamps,
     }
     __syncthreads();
   }
+  // every lane of every warp gets here (the loops above are uniform across a warp)
+  if (special != nullptr && __any_sync(0xffffffffu, odd) && tx == 0) atomicOr(special, 1u);
 }
 
 // Per-sample zero-DM sums zdm[t] = sum_c f64(x[t][c]) (one warp per sample).
@@ -287,6 +310,10 @@ struct DmtArgs {
   int64_t out_start;
   int64_t nvalid;
   uint32_t* status;
+  // float64 accumulation of float32 rows: a word that is 0 when every sample
+  // of the block is a normal float32 (set by the corner turn); then part of
+  // the conversions run on the integer pipe.  nullptr: conversion unit only.
+  const uint32_t* special;
 };
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES>
@@ -402,6 +429,12 @@ k_dmt(const DmtArgs a) {
     double d_acc[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) { s_acc[r] = 0.f; c_acc[r] = 0.f; d_acc[r] = 0.0; }
+    // all samples normal: one word in four converts by field arithmetic
+    // (integer pipe), the rest by F2F (conversion unit): exactly the same
+    // values.  F2F alone keeps the conversion unit near full; the field
+    // conversion costs ~6 issue slots, so half and half made the kernel
+    // issue-bound at the same speed and one in four is the balance measured.
+    const bool split = ACC == SPP_ACC_F64 && a.special != nullptr && *a.special == 0u;
     for (int k = 0; k < nslab; ++k) {
       const int s = k % STAGES;
       if (!mbar_wait(&full[s], (k / STAGES) & 1, a.status)) { ok = false; break; }
@@ -413,14 +446,26 @@ k_dmt(const DmtArgs a) {
       float p_acc[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) p_acc[r] = 0.f;
+      if (ACC == SPP_ACC_F64 && split) {
 #pragma unroll 4
-      for (int j = 0; j < nc; ++j) {
-        const float* row = sd + j * a.slot_w + (wbase + dl[j]);
+        for (int j = 0; j < nc; ++j) {
+          const float* row = sd + j * a.slot_w + (wbase + dl[j]);
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const float x = row[32 * r];
-          if (ACC == SPP_ACC_F64) d_acc[r] += (double)x;
-          else p_acc[r] = __fadd_rn(p_acc[r], x);
+          for (int r = 0; r < R; ++r) {
+            const float x = row[32 * r];
+            d_acc[r] += (r % 4 == 3) ? f64_of_normal_f32(x) : (double)x;
+          }
+        }
+      } else {
+#pragma unroll 4
+        for (int j = 0; j < nc; ++j) {
+          const float* row = sd + j * a.slot_w + (wbase + dl[j]);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const float x = row[32 * r];
+            if (ACC == SPP_ACC_F64) d_acc[r] += (double)x;
+            else p_acc[r] = __fadd_rn(p_acc[r], x);
+          }
         }
       }
       if (ACC != SPP_ACC_F64) {

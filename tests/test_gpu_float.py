@@ -118,3 +118,34 @@ def test_config5_geometry(orc):
                     assert rep["max_err_over_bound"] <= 1.0, (v, rep)
             plan.close()
     print("per-result error vs float64:", reports)
+
+
+@pytest.mark.parametrize("plant", ["none", "zero", "subnormal", "inf"])
+def test_f64_conversion_paths(orc, plant):
+    """Float64 sums convert every other float32 by field arithmetic when the
+    corner turn saw only normal floats, and through the conversion unit alone
+    otherwise (a zero, a subnormal or an infinity anywhere in the block):
+    both give the oracle's bits."""
+    import torch
+
+    from sigpyproc3_b200 import _lib
+    from sigpyproc3_b200.dedisp import DMTPlan
+    from sigpyproc3_b200.header import Header
+
+    nchans, nsamps = 256, 6000
+    h = Header(nchans=nchans, fch1=1400.0, foff=-0.5, tsamp=64e-6, nbits=32)
+    d = np.atleast_2d(h.get_dmdelays(np.linspace(0, 200, 24))).astype(np.int32)
+    rng = np.random.default_rng(77)
+    x = rng.normal(0.0, 1.0, size=(nsamps, nchans)).astype(np.float32)
+    value = {"zero": 0.0, "subnormal": 1e-40, "inf": np.inf}.get(plant)
+    if value is not None:
+        x[2500, 100] = np.float32(value)
+    nv = nsamps - int(d.max())
+    ref32 = orc.dmt(x.ravel(), d, nchans, nsamps, nv)
+    plan = DMTPlan(d, nchans, nsamps, nbits=32, acc=_lib.ACC_F64)
+    xd = torch.from_numpy(x.ravel()).cuda()
+    for v in range(plan.num_variants):
+        plan.set_variant(v)
+        out = plan.execute(xd, nsamps).cpu().numpy()
+        np.testing.assert_array_equal(out, ref32, err_msg=f"{plan.describe()} {plant}")
+    plan.close()
