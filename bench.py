@@ -434,7 +434,10 @@ def main():
                     help="config 5: float accumulator")
     ap.add_argument("--no-secondary", action="store_true", help="skip the config 1/3 blocks")
     ap.add_argument("--variant", type=int, default=None, help="fix the kernel variant")
-    ap.add_argument("--workload", choices=["c2", "c3", "c4", "c1", "c5", "snr", "fold"], default="c2")
+    ap.add_argument("--workload", choices=["c2", "c3", "c4", "c1", "c5", "snr", "fold", "dmt"],
+                    default="c2")
+    ap.add_argument("--nbits", type=int, default=2, choices=[1, 2, 4, 8],
+                    help="--workload dmt: sample width")
     ap.add_argument("--beams", type=int, default=64, help="config 3: number of beams")
     ap.add_argument("--batch", type=int, default=4, help="config 3: beams per graph")
     ap.add_argument("--chunks", type=int, default=128, help="config 4: chunks served")

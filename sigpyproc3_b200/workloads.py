@@ -1,5 +1,5 @@
 """Benchmark workloads other than the default DM-time transform (bench.py
---workload c1|c3|c4|c5|snr|fold).  Each prints one JSON line through ``emit``;
+--workload c1|c3|c4|c5|snr|fold|dmt).  Each prints one JSON line through ``emit``;
 ``measure_c1`` and ``measure_c3`` also feed the secondary blocks of the
 default line."""
 
@@ -24,7 +24,7 @@ def run(name: str, args, rank: int, world: int, local: int, emit, checks=None) -
     """Run one workload; ``checks`` maps a workload name to a correctness
     checker the caller supplies (run outside the timed region)."""
     fn = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "snr": run_snr,
-          "fold": run_fold}[name]
+          "fold": run_fold, "dmt": run_dmt}[name]
     if name == "c5":
         fn(args, rank, world, local, emit, checks or {})
     else:
@@ -497,6 +497,57 @@ def run_snr(args, rank, world, local, emit) -> None:
              roofline={"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak,
                        "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak,
                        "algorithmic_bytes": alg})
+
+
+def run_dmt(args, rank, world, local, emit) -> None:
+    """DM-time transform of one block of seeded uniform samples of any width
+    on the config-2 band (4096 channels from 1500 MHz down 300 MHz, 64 us):
+    ``--nbits`` 1/2/4/8, ``--ndm`` trials (a contiguous block from the middle
+    of the dmt_transform(1000, 1024) grid; all 1024 by default), ``--nsamps``
+    output samples (2^18 by default).  Every kernel variant the plan accepts
+    is timed (``--variant`` fixes one), corner turn and DM-time kernel
+    separately; the line's value is the fastest kernel's channel-adds/s.
+    For comparing the SIMD and bit-sliced kernels, and as the command of
+    kernel captures."""
+    from .dedisp import DMTPlan
+
+    g = synth.C2
+    nb = args.nbits
+    ndm = args.ndm or 1024
+    nout = args.nsamps or (1 << 18)
+    lo = (1024 - ndm) // 2
+    d = np.atleast_2d(g.delays(synth.dm_grid(1000.0, 1024)[lo:lo + ndm])).astype(np.int32)
+    nsamps = nout + int(d.max())
+    raw = synth.uniform_bytes_device(nsamps * g.nchans * nb // 8, 7)
+    out = torch.empty((ndm, nout), dtype=torch.int32, device="cuda")
+    plan = DMTPlan(d, g.nchans, nsamps, nbits=nb, bitorder="little" if nb == 1 else "big",
+                   out_dtype=torch.int32)
+    steps = max(args.steps, 1)
+    rows = []
+    for v in range(plan.num_variants) if args.variant is None else [args.variant]:
+        plan.set_variant(v)
+        for _ in range(max(args.warmup, 1)):
+            plan.execute(raw, nsamps, out)
+        torch.cuda.synchronize()
+        plan.timing(True)
+        for _ in range(steps):
+            plan.execute(raw, nsamps, out)
+        t = plan.timing_read()
+        plan.timing(False)
+        ms = t["ms_dmt"] / steps
+        rows.append({"variant": v, "ms_dmt": ms, "ms_corner_turn": t["ms_corner_turn"] / steps,
+                     "adds_per_s": ndm * nout * g.nchans / (ms / 1e3), **plan.describe()})
+    plan.close()
+    best = max(rows, key=lambda r: r["adds_per_s"])
+    if rank == 0:
+        emit(metric="channel-adds/s, DM-time kernel (kernel comparison)",
+             value=best["adds_per_s"], unit="adds/s", n_gpus=world, steps=steps,
+             warmup=args.warmup, ms_per_step=best["ms_dmt"], higher_is_better=True,
+             scaling="weak", vs_baseline=None, dtype=f"u{nb}->int32",
+             data="synthetic uniform bytes on device (seed 7)",
+             config={"workload": f"DM-time transform, {nb}-bit 4096 ch x {nout} outputs, "
+                     f"{ndm} trials of dmt_transform(1000, 1024) (config-2 band)",
+                     "variants": rows})
 
 
 def run_fold(args, rank, world, local, emit) -> None:
