@@ -71,6 +71,15 @@ int spp_version(void);
 int spp_status_read(const void* workspace, uint32_t* host_out, void* stream);
 int spp_status_clear(void* workspace, void* stream);
 
+/* Page-lock (and release) host memory that already holds a filterbank, so
+ * blocks are copied to the GPU by DMA straight from it instead of through a
+ * staging buffer (the reference reads each block into a host buffer,
+ * io/fileio.py:234-296; there is no device side to copy to).  A refused
+ * registration (memory already registered, too large) returns SPP_ERR_CUDA
+ * and leaves no pending CUDA error behind. */
+int spp_host_register(void* ptr, int64_t bytes);
+int spp_host_unregister(void* ptr);
+
 /* ---- R4: unpack -------------------------------------------------------------
  * Replaces kernels.unpack{1,2,4}_8_{big,little} (core/kernels.py:20-69) and
  * io/bits.py unpack (:19-70): `nbytes` packed bytes -> nbytes*8/nbits uint8

@@ -43,6 +43,8 @@ SIGNATURES: dict[str, tuple[list, object]] = {
     "spp_version": ([], _int),
     "spp_status_read": ([_p, _p, _p], _int),
     "spp_status_clear": ([_p, _p], _int),
+    "spp_host_register": ([_p, _i64], _int),
+    "spp_host_unregister": ([_p], _int),
     "spp_unpack": ([_p, _i64, _int, _int, _p, _p], _int),
     "spp_dedisperse_workspace_bytes": ([_int, _i64, _i64, _i32, _i32], _i64),
     "spp_dedisperse": ([_p, _int, _int, _i64, _i64, _p, _i32, _i32, _p, _i64, _i64, _int, _p,

@@ -316,6 +316,26 @@ int spp_status_clear(void* workspace, void* stream) {
   return cuda_status(cudaMemsetAsync(workspace, 0, 16, as_stream(stream)), "status clear");
 }
 
+int spp_host_register(void* ptr, int64_t bytes) {
+  if (!ptr || bytes <= 0) return fail(SPP_ERR_ARG, "spp_host_register: null pointer or size <= 0");
+  const cudaError_t e = cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterPortable);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // a refused registration must not surface at the next launch check
+    return fail(SPP_ERR_CUDA, "cudaHostRegister: %s", cudaGetErrorString(e));
+  }
+  return SPP_OK;
+}
+
+int spp_host_unregister(void* ptr) {
+  if (!ptr) return fail(SPP_ERR_ARG, "spp_host_unregister: null pointer");
+  const cudaError_t e = cudaHostUnregister(ptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(SPP_ERR_CUDA, "cudaHostUnregister: %s", cudaGetErrorString(e));
+  }
+  return SPP_OK;
+}
+
 int spp_unpack(const uint8_t* in, int64_t nbytes, int nbits, int bitorder, uint8_t* out,
                void* stream) {
   if (nbytes < 0) return fail(SPP_ERR_ARG, "nbytes < 0");

@@ -11,6 +11,7 @@ identical block for block.
 
 from __future__ import annotations
 
+import warnings
 from collections.abc import Callable, Iterator
 from pathlib import Path
 
@@ -45,6 +46,10 @@ def plan_blocks(nsamples: int, gulp: int, start: int, nsamps: int | None,
     if lastread != 0:
         blocks.append((nreads, lastread, 0))
     return gulp, blocks
+
+
+# In-memory filterbanks up to this size are page-locked in place on first use.
+REGISTER_MAX_BYTES = 8 << 30
 
 
 def pinned_allocator(nbytes: int) -> torch.Tensor:
@@ -92,6 +97,12 @@ class Filterbank:
     def _read_bytes(self, offset: int, view: np.ndarray) -> int:  # pragma: no cover
         raise NotImplementedError
 
+    def _device_source(self, offset: int, nbytes: int) -> torch.Tensor | None:
+        """Bytes [offset, offset + nbytes) as a page-locked host tensor the GPU
+        can copy from directly, or None: blocks are staged through pinned
+        buffers filled by ``_read_bytes``."""
+        return None
+
     # --- streaming (R5) ---
     def stream_blocks(self, gulp: int = 16384, start: int = 0, nsamps: int | None = None,
                       skipback: int = 0, *, allocator: Callable[[int], object] | None = None,
@@ -108,8 +119,13 @@ class Filterbank:
         nbytes = gulp * rb
         alloc = pinned_allocator if allocator is None else allocator
         dev = torch.device("cuda", torch.cuda.current_device())
-        host = [_allocate(alloc, nbytes) for _ in range(2)]
-        hviews = [_host_view(h) for h in host]
+        # data already in page-locked host memory is copied straight from
+        # there (default allocator only: a caller's allocator is always used)
+        direct = allocator is None and self._device_source(0, 0) is not None
+        host = hviews = None
+        if not direct:
+            host = [_allocate(alloc, nbytes) for _ in range(2)]
+            hviews = [_host_view(h) for h in host]
         devbuf = [torch.empty(nbytes, dtype=torch.uint8, device=dev) for _ in range(2)]
         copy_stream = torch.cuda.Stream(dev)
         compute = torch.cuda.current_stream(dev)
@@ -120,18 +136,24 @@ class Filterbank:
         for ii, nsamp_blk, skip in blocks:
             k = ii & 1
             want = nsamp_blk * rb
-            if used[k]:
-                copied[k].synchronize()  # host buffer k is free once its copy landed
-            got = self._read_bytes(pos, hviews[k][:want])
-            if got != want:
-                raise ValueError(f"Unexpected number of bytes read from file {got} (actual) "
-                                 f"!= {want} (expected)")
+            src = self._device_source(pos, want) if direct else None
+            if src is None:
+                if direct:
+                    got = max(0, min(want, self._raw.nbytes - pos))
+                    raise ValueError(f"Unexpected number of bytes read from file {got} (actual) "
+                                     f"!= {want} (expected)")
+                if used[k]:
+                    copied[k].synchronize()  # host buffer k is free once its copy landed
+                got = self._read_bytes(pos, hviews[k][:want])
+                if got != want:
+                    raise ValueError(f"Unexpected number of bytes read from file {got} (actual) "
+                                     f"!= {want} (expected)")
+                src = (host[k] if torch.is_tensor(host[k]) else torch.from_numpy(hviews[k]))[:want]
             pos += want + skip * rb
             with torch.cuda.stream(copy_stream):
                 if used[k]:
                     copy_stream.wait_event(consumed[k])
-                src = host[k] if torch.is_tensor(host[k]) else torch.from_numpy(hviews[k])
-                devbuf[k][:want].copy_(src[:want], non_blocking=True)
+                devbuf[k][:want].copy_(src, non_blocking=True)
                 copied[k].record(copy_stream)
             compute.wait_event(copied[k])
             used[k] = True
@@ -521,11 +543,18 @@ class FilReader(Filterbank):
 
 
 class ArrayFilterbank(Filterbank):
-    """A filterbank held in host memory (raw time-major bytes), e.g. synthetic data."""
+    """A filterbank held in host memory (raw time-major bytes), e.g. synthetic data.
+
+    On first use the array (up to REGISTER_MAX_BYTES) is page-locked in place,
+    so each block is copied to the GPU by DMA straight from it rather than
+    through a staging buffer; it is released when the object is collected.
+    If the driver refuses (e.g. the memory is already registered elsewhere),
+    blocks are staged as for files."""
 
     def __init__(self, raw: np.ndarray, header: Header):
         self._raw = np.ascontiguousarray(raw).view(np.uint8).ravel()
         self._header = header
+        self._registered: bool | None = None  # None: not tried yet
 
     @property
     def header(self) -> Header:
@@ -535,6 +564,24 @@ class ArrayFilterbank(Filterbank):
         n = max(0, min(view.nbytes, self._raw.nbytes - offset))
         view[:n] = self._raw[offset:offset + n]
         return n
+
+    def _device_source(self, offset: int, nbytes: int) -> torch.Tensor | None:
+        if self._registered is None:
+            n = self._raw.nbytes
+            self._registered = (0 < n <= REGISTER_MAX_BYTES and
+                                _lib.load().spp_host_register(self._raw.ctypes.data, n) == 0)
+        if not self._registered or offset + nbytes > self._raw.nbytes:
+            return None
+        with warnings.catch_warnings():  # read-only arrays: the view is only read
+            warnings.simplefilter("ignore", UserWarning)
+            return torch.from_numpy(self._raw[offset:offset + nbytes])
+
+    def __del__(self):
+        if getattr(self, "_registered", False):
+            try:
+                _lib.load().spp_host_unregister(self._raw.ctypes.data)
+            except Exception:  # interpreter shutdown
+                pass
 
 
 class PulseExtractor:
