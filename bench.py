@@ -13,14 +13,15 @@ input already resident in HBM.  The input (1 GiB) and output (4.2 GB) exceed
 L2, so no flush is needed between steps.  The same line carries the
 end-to-end rate through the C ABI from pinned host memory (``e2e``), a
 bit-exact check of whole rows of that end-to-end output against the CPU oracle
-(``parity``), the CPU baseline, and secondary blocks for configs 1 and 3.
+(``parity``), the CPU baseline, and secondary blocks for configs 1, 3 and 4.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 Under torchrun each rank runs an independent replica of the workload (the
 path shards without any exchange); the timed region is bracketed by a
 barrier and device synchronisation, and the elapsed time is the maximum over
-ranks.  --impl reference times the CPU restatement of the reference loop
+ranks; the end-to-end leg likewise runs on every rank after a barrier and
+takes the slowest rank's time.  --impl reference times the CPU restatement of the reference loop
 (oracle/: the reference is Python + numba, whose source does not travel to
 the GPU host) on a bounded sample of the same workload, on rank 0 only; that
 arm imports neither torch nor this repository's CUDA library.
@@ -327,7 +328,9 @@ def run_gpu(args, rank, world, local):
     e2e = None
     cpu = None
     parity = None
-    if rank == 0 and not args.no_e2e:
+    if not args.no_e2e:
+        # every rank streams its own copy through its GPU; the job's time is
+        # the slowest rank's (collectives in the same order on every rank)
         host_in = torch.empty(raw.numel(), dtype=torch.uint8).pin_memory()
         host_in.copy_(raw.cpu())
         host_out = torch.empty((delays.shape[0], nvalid), dtype=torch.int32).pin_memory()
@@ -337,23 +340,25 @@ def run_gpu(args, rank, world, local):
         torch.cuda.empty_cache()
         plan.execute_host(host_in.numpy(), g.nsamps, host_out.numpy(), block_nsamps=blk, ws=hws)
         ne = max(1, min(args.steps, 3))
+        _barrier(world)
         t0 = time.perf_counter()
         for _ in range(ne):
             plan.execute_host(host_in.numpy(), g.nsamps, host_out.numpy(), block_nsamps=blk,
                               ws=hws)
         t1 = time.perf_counter()
+        t_step = multi.max_over_ranks((t1 - t0) / ne * 1e3) / 1e3
         nblk = -(-nvalid // blk)
         h2d = sum((min(blk, nvalid - b * blk) + int(delays.max())) * g.nchans * g.nbits // 8
                   for b in range(nblk))
-        e2e = {"value": delays.shape[0] * nvalid / ((t1 - t0) / ne), "unit": UNIT,
+        e2e = {"value": world * delays.shape[0] * nvalid / t_step, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(delays.shape[0] * nvalid * 4),
                "steps": ne, "path": "spp_dmt_execute_host (C ABI), pinned host buffers"}
         # whole rows of the end-to-end output against the oracle (outside timing)
-        if not args.no_parity:
+        if rank == 0 and not args.no_parity:
             prow = np.unique(np.linspace(0, delays.shape[0] - 1, 8).astype(int))
             parity = e2e_parity(g.nchans, g.nbits, g.nsamps, delays, host_in.numpy(),
                                 host_out.numpy(), nvalid, prow)
-        if world == 1 and not args.no_cpu:
+        if rank == 0 and world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
             rows = 65536 + int(delays.max())
             rb = g.nchans * g.nbits // 8
