@@ -103,6 +103,11 @@ class Filterbank:
         buffers filled by ``_read_bytes``."""
         return None
 
+    def _bytes_available(self, offset: int, nbytes: int) -> int:
+        """How many of the bytes [offset, offset + nbytes) exist (sources with
+        a direct path report it when a block runs past the data)."""
+        return 0
+
     # --- streaming (R5) ---
     def stream_blocks(self, gulp: int = 16384, start: int = 0, nsamps: int | None = None,
                       skipback: int = 0, *, allocator: Callable[[int], object] | None = None,
@@ -139,7 +144,7 @@ class Filterbank:
             src = self._device_source(pos, want) if direct else None
             if src is None:
                 if direct:
-                    got = max(0, min(want, self._raw.nbytes - pos))
+                    got = self._bytes_available(pos, want)
                     raise ValueError(f"Unexpected number of bytes read from file {got} (actual) "
                                      f"!= {want} (expected)")
                 if used[k]:
@@ -564,6 +569,9 @@ class ArrayFilterbank(Filterbank):
         n = max(0, min(view.nbytes, self._raw.nbytes - offset))
         view[:n] = self._raw[offset:offset + n]
         return n
+
+    def _bytes_available(self, offset: int, nbytes: int) -> int:
+        return max(0, min(nbytes, self._raw.nbytes - offset))
 
     def _device_source(self, offset: int, nbytes: int) -> torch.Tensor | None:
         if self._registered is None:
