@@ -331,7 +331,10 @@ int spp_boxcar_snr_robust(const void* in, int in_kind, int64_t nrows,
  * stats.estimate_zscore (core/stats.py:418-502) into loc_scale[row * 2 + 0/1]
  * (device float64): method 0 = mean / population std, method 1 = median
  * (float32, the two middle values averaged in float32) / IQR / 1.349 (exact
- * order statistics); a scale within 1e-8 of 0 becomes 1.
+ * order statistics), method 2 = the same median / stats._scale_mad
+ * (core/stats.py:505-536: median absolute deviation from the float64 median
+ * / 0.6745, exact order statistics; the mean absolute deviation / sqrt(2/pi)
+ * when that is within 1e-8 of 0); a scale within 1e-8 of 0 becomes 1.
  * spp_zscore: out[i] = f32(f64(f32(in[i] - f32(loc))) / scale), the rounding
  * of np.subtract(..., dtype=float32) then np.divide into float32.
  * spp_matched_filter: kernels.convolve_templates (core/kernels.py:861-906)

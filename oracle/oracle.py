@@ -344,6 +344,18 @@ def filterbank_fold(data: np.ndarray, nsamples: int, nchans: int, delays: np.nda
 # real transforms (scipy.fft.next_fast_len(n, real=True): the same pocketfft
 # rule the reference reaches through rocket_fft.good_size).
 # ---------------------------------------------------------------------------
+def mad_scale(x: np.ndarray) -> float:
+    """stats._scale_mad (core/stats.py:505-536): the median absolute deviation
+    from the float64 median over Phi^-1(3/4); when that is within 1e-8 of 0,
+    the mean absolute deviation over sqrt(2/pi)."""
+    d = np.asarray(x, dtype=np.float64)
+    loc = np.median(d)
+    mad = np.median(np.abs(d - loc)) / 0.6744897501960817
+    if np.isclose(mad, 0):
+        mad = np.mean(np.abs(d - loc)) / np.sqrt(2 / np.pi)
+    return float(mad)
+
+
 def zscore_f32(x: np.ndarray, loc_method: str, scale_method: str):
     """stats.estimate_zscore (core/stats.py:418-477) on a float32 series."""
     x = np.asarray(x, dtype=np.float32)
@@ -360,6 +372,8 @@ def zscore_f32(x: np.ndarray, loc_method: str, scale_method: str):
         scale = np.float64((q[1] - q[0]) / 1.3489795003921634)
     elif scale_method == "std":
         scale = np.float64(np.std(x.astype(np.float64)))
+    elif scale_method == "mad":
+        scale = np.float64(mad_scale(x))
     else:
         scale = np.float32(1.0)
     if np.isclose(scale, 0):

@@ -137,6 +137,16 @@ def load_read_plan():
     return ns["read_plan"]
 
 
+def load_scale_mad():
+    """Reference ``stats._scale_mad`` (core/stats.py:505-536), executed as-is."""
+    import numpy as np
+
+    src = _extract(SRC / "core" / "stats.py", {"_scale_mad"})
+    ns: dict = {"np": np, "NDArray": object}
+    exec(compile("from __future__ import annotations\n" + src, "stats.py", "exec"), ns)
+    return ns["_scale_mad"]
+
+
 def load_scale_iqr():
     """Reference ``stats._scale_iqr`` (core/stats.py:480-502), executed as-is."""
     import numpy as np

@@ -940,6 +940,128 @@ static int boxcar_snr_impl(const void* in, int in_kind, int64_t nrows, int64_t n
   return cuda_status(cudaGetLastError(), "snr final launch");
 }
 
+// ---------------------------------------------------------------------------
+// Median absolute deviation of each row (stats._scale_mad, core/stats.py:
+// 505-536, with estimate_loc's float32 median, core/stats.py:284-326).  One
+// CTA per row: the two middle values by radix selection over order-preserving
+// 32-bit float keys give the float32 median (averaged in float32) and the
+// float64 one (averaged in float64, as np.median of the float64 copy); the
+// two middle absolute deviations |f64(x) - median64| by radix selection over
+// their 64-bit patterns (non-negative doubles order as unsigned integers) give
+// the MAD, divided by Phi^-1(3/4); a MAD within 1e-8 of 0 is replaced by the
+// mean absolute deviation over sqrt(2/pi) (a float64 sum in another order
+// than numpy's pairwise one), and a scale within 1e-8 of 0 by 1.
+// ---------------------------------------------------------------------------
+
+// Ranks r0 <= r1 of n keys by radix selection in one CTA: digits of kQBits
+// from the top; each pass histograms (warp-aggregated shared atomics) the
+// keys that match a rank's fixed higher digits, then fixes that rank's next
+// digit.  `out` (shared) receives the two keys.
+template <typename K, class KeyF>
+__device__ void select_pair(int64_t n, int64_t r0, int64_t r1, const KeyF& key, uint32_t* hist,
+                            K* out) {
+  constexpr int kBits = (int)sizeof(K) * 8;
+  __shared__ K pre[2];
+  __shared__ long long rk[2];
+  if (threadIdx.x == 0) {
+    pre[0] = pre[1] = K(0);
+    rk[0] = r0;
+    rk[1] = r1;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int hi = kBits; hi > 0; hi -= kQBits) {
+    const int lo = hi > kQBits ? hi - kQBits : 0;
+    const int wb = hi - lo;
+    const K himask = hi >= kBits ? K(0) : ~((K(1) << hi) - K(1));
+    const K dmask = (K(1) << wb) - K(1);
+    for (int i = threadIdx.x; i < 2 * kQBins; i += blockDim.x) hist[i] = 0u;
+    __syncthreads();
+    const K p0 = pre[0], p1 = pre[1];
+    const int64_t nr = (n + blockDim.x - 1) / blockDim.x * blockDim.x;  // whole warps iterate
+    for (int64_t i = threadIdx.x; i < nr; i += blockDim.x) {
+      int id0 = -1, id1 = -1;
+      if (i < n) {
+        const K k = key(i);
+        const int dig = (int)((k >> lo) & dmask);
+        if ((k & himask) == p0) id0 = dig;
+        if ((k & himask) == p1) id1 = kQBins + dig;
+      }
+      unsigned peers = __match_any_sync(0xffffffffu, id0);
+      if (id0 >= 0 && lane == __ffs(peers) - 1) atomicAdd(&hist[id0], (uint32_t)__popc(peers));
+      peers = __match_any_sync(0xffffffffu, id1);
+      if (id1 >= 0 && lane == __ffs(peers) - 1) atomicAdd(&hist[id1], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      const int r = threadIdx.x;
+      const uint32_t* h = hist + r * kQBins;
+      long long c = 0;
+      int d = 0;
+      for (; d < (1 << wb) - 1; ++d) {
+        if (rk[r] < c + (long long)h[d]) break;
+        c += h[d];
+      }
+      rk[r] -= c;
+      pre[r] |= K(d) << lo;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = pre[0];
+    out[1] = pre[1];
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kQThreads)
+k_row_mad(const void* __restrict__ in, int kind, int64_t n, int64_t in_stride,
+          double* __restrict__ locscale) {
+  __shared__ uint32_t hist[2 * kQBins];
+  __shared__ uint32_t k32[2];
+  __shared__ unsigned long long k64[2];
+  __shared__ double red[kQThreads / 32];
+  const int64_t row = blockIdx.x;
+  const char* base = static_cast<const char*>(in) + row * in_stride * 4;
+  // the reference z-scores float32 data (integer rows converted exactly)
+  auto xv = [&](int64_t i) -> float {
+    return kind == SPP_OUT_I32 ? (float)reinterpret_cast<const int32_t*>(base)[i]
+                               : reinterpret_cast<const float*>(base)[i];
+  };
+  const int64_t r0 = (n - 1) / 2, r1 = n / 2;
+  select_pair<uint32_t>(n, r0, r1, [&](int64_t i) { return f32_key(xv(i)); }, hist, k32);
+  const float a = key_f32(k32[0]), b = key_f32(k32[1]);
+  const float med32 = (n & 1) ? a : __fmul_rn(__fadd_rn(a, b), 0.5f);
+  const double med64 = (n & 1) ? (double)a : __dmul_rn(__dadd_rn((double)a, (double)b), 0.5);
+  select_pair<unsigned long long>(
+      n, r0, r1,
+      [&](int64_t i) {
+        return (unsigned long long)__double_as_longlong(fabs(__dsub_rn((double)xv(i), med64)));
+      },
+      hist, k64);
+  const double da = __longlong_as_double((long long)k64[0]);
+  const double db = __longlong_as_double((long long)k64[1]);
+  const double medd = (n & 1) ? da : __dmul_rn(__dadd_rn(da, db), 0.5);
+  double mad = __ddiv_rn(medd, 0.6744897501960817);  // scipy.stats.norm.ppf(0.75)
+  if (fabs(mad) <= 1e-8) {  // np.isclose(mad, 0)
+    double s = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) s += fabs(__dsub_rn((double)xv(i), med64));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < kQThreads / 32; ++w) t += red[w];
+      mad = __ddiv_rn(__ddiv_rn(t, (double)n), __dsqrt_rn(__ddiv_rn(2.0, 3.141592653589793)));
+    }
+  }
+  if (threadIdx.x == 0) {
+    locscale[row * 2] = (double)med32;
+    locscale[row * 2 + 1] = fabs(mad) <= 1e-8 ? 1.0 : mad;
+  }
+}
+
 extern "C" {
 
 int spp_boxcar_snr(const void* in, int in_kind, int64_t nrows, int64_t n, int64_t in_stride,
@@ -981,7 +1103,12 @@ int spp_row_loc_scale(const void* in, int in_kind, int64_t nrows, int64_t n, int
     k_row_mean_std<<<(unsigned)nrows, 256, 0, st>>>(in, in_kind, n, in_stride, loc_scale);
     return cuda_status(cudaGetLastError(), "mean/std launch");
   }
-  if (method != 1) return fail(SPP_ERR_ARG, "method must be 0 (mean/std) or 1 (median/iqr)");
+  if (method == 2) {
+    k_row_mad<<<(unsigned)nrows, kQThreads, 0, st>>>(in, in_kind, n, in_stride, loc_scale);
+    return cuda_status(cudaGetLastError(), "median/MAD launch");
+  }
+  if (method != 1)
+    return fail(SPP_ERR_ARG, "method must be 0 (mean/std), 1 (median/iqr) or 2 (median/mad)");
   SnrCfg cfg{};
   cfg.nf = 1;
   cfg.f[0] = 1;

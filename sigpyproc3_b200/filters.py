@@ -152,9 +152,9 @@ class MatchedFilter:
             raise ValueError(f"Data dimension {x.dim()} is not supported.")
         if loc_method not in {"median", "mean", "norm"}:
             raise ValueError(f"Method {loc_method} is not supported for estimating location.")
-        if scale_method not in {"iqr", "std", "norm"}:
+        if scale_method not in {"iqr", "mad", "std", "norm"}:
             raise NotImplementedError(f"scale_method {scale_method!r} is not on the GPU path "
-                                      "(iqr, std or norm)")
+                                      "(iqr, mad, std or norm)")
         if temp_kind not in {"boxcar", "gaussian", "lorentzian"}:
             raise ValueError(f"unknown template kind {temp_kind!r}")
         if x.numel() == 0:
@@ -243,10 +243,14 @@ class MatchedFilter:
         if "mean" == loc_method or "std" == scale_method:
             _lib.check(lib.spp_row_loc_scale(self._x.data_ptr(), _lib.OUT_F32, 1, n, n, 0,
                                              plain.data_ptr(), st))
+        mad = torch.empty(2, dtype=torch.float64, device=self._x.device)
+        if scale_method == "mad":
+            _lib.check(lib.spp_row_loc_scale(self._x.data_ptr(), _lib.OUT_F32, 1, n, n, 2,
+                                             mad.data_ptr(), st))
         if loc_method != "norm":
             ls[0] = (robust if loc_method == "median" else plain)[0]
         if scale_method != "norm":
-            ls[1] = (robust if scale_method == "iqr" else plain)[1]
+            ls[1] = {"iqr": robust, "mad": mad, "std": plain}[scale_method][1]
         self._z = torch.empty_like(self._x)
         _lib.check(lib.spp_zscore(self._x.data_ptr(), n, ls.data_ptr(), self._z.data_ptr(), st))
         host = ls.cpu().numpy()

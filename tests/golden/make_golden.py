@@ -304,12 +304,21 @@ def main() -> None:
     # ---- R9 robust z-score: np.median and the reference's _scale_iqr
     # (core/stats.py:418-502, MatchedFilter's defaults) on seeded series
     scale_iqr = refload.load_scale_iqr()
+    scale_mad = refload.load_scale_mad()
     zs = []
     rng = np.random.default_rng(17)
     for k, m in enumerate((1, 2, 7, 8, 1000, 1001, 65536)):
         y = (rng.normal(3.0, 2.0, m) if k % 2 else rng.integers(0, 9, m)).astype(np.float32)
         out[f"zscore_in_{k}"] = y
-        zs.append({"m": m, "median": float(np.median(y)), "iqr_scale": float(scale_iqr(y))})
+        zs.append({"m": m, "median": float(np.median(y)), "iqr_scale": float(scale_iqr(y)),
+                   "mad_scale": float(scale_mad(y))})
+    # two thirds of the samples equal to the median: MAD 0, so the reference's
+    # _scale_mad falls back to the mean absolute deviation
+    y = np.full(999, 5.0, dtype=np.float32)
+    y[::3] = rng.normal(5.0, 2.0, 333).astype(np.float32)
+    out[f"zscore_in_{len(zs)}"] = y
+    zs.append({"m": 999, "median": float(np.median(y)), "iqr_scale": float(scale_iqr(y)),
+               "mad_scale": float(scale_mad(y))})
     meta["zscore"] = zs
 
     # ---- N2 kernels.downsample_2d_mean_flat (core/kernels.py:207-252) on

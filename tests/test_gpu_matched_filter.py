@@ -21,7 +21,7 @@ def torch_cuda():
 
 @pytest.mark.parametrize("kind", ["boxcar", "gaussian", "lorentzian"])
 @pytest.mark.parametrize("loc,scale", [("median", "iqr"), ("mean", "std"), ("median", "std"),
-                                       ("norm", "norm")])
+                                       ("norm", "norm"), ("median", "mad"), ("mean", "mad")])
 def test_matched_filter_vs_oracle(torch_cuda, orc, kind, loc, scale):
     from sigpyproc3_b200.filters import MatchedFilter
 
@@ -57,3 +57,27 @@ def test_matched_filter_edges(torch_cuda, orc):
         MatchedFilter(np.zeros(10, np.float32), temp_kind="gaussian", nbins_max=32)
     with pytest.raises(ValueError):
         MatchedFilter(np.zeros((2, 10), np.float32))
+
+
+def test_row_loc_scale_mad_matches_reference(torch_cuda, golden, golden_meta):
+    """spp_row_loc_scale method 2 on the recorded series: the float32 median
+    and the reference's own stats._scale_mad values (golden) -- exact order
+    statistics, so equal to the last bit; the mean-absolute-deviation branch
+    (MAD 0) sums in another order than numpy, so within 1e-12 there."""
+    torch = torch_cuda
+    from sigpyproc3_b200 import _lib
+
+    lib = _lib.load()
+    for k, rec in enumerate(golden_meta["zscore"]):
+        y = torch.from_numpy(golden[f"zscore_in_{k}"]).cuda()
+        ls = torch.empty(2, dtype=torch.float64, device="cuda")
+        _lib.check(lib.spp_row_loc_scale(y.data_ptr(), _lib.OUT_F32, 1, y.numel(), y.numel(), 2,
+                                         ls.data_ptr(), torch.cuda.current_stream().cuda_stream))
+        loc, scale = ls.cpu().numpy()
+        assert loc == rec["median"], (k, loc, rec)
+        expect = rec["mad_scale"] if not np.isclose(rec["mad_scale"], 0) else 1.0
+        d = golden[f"zscore_in_{k}"].astype(np.float64)
+        if np.isclose(np.median(np.abs(d - np.median(d))), 0) and expect != 1.0:
+            assert scale == pytest.approx(expect, rel=1e-12), (k, scale, rec)
+        else:
+            assert scale == expect, (k, scale, rec)

@@ -160,6 +160,19 @@ def test_robust_zscore_matches_reference(orc, golden, golden_meta):
         assert scale == expect, (k, scale, rec)
 
 
+def test_mad_scale_matches_reference(orc, golden, golden_meta):
+    """The oracle's MAD scale equals the reference's stats._scale_mad
+    (core/stats.py:505-536) on the recorded series, including those whose MAD
+    is 0 (mean absolute deviation instead)."""
+    zero = 0
+    for k, rec in enumerate(golden_meta["zscore"]):
+        y = golden[f"zscore_in_{k}"]
+        assert orc.mad_scale(y) == rec["mad_scale"], (k, rec)
+        d = y.astype(np.float64)
+        zero += bool(np.isclose(np.median(np.abs(d - np.median(d))), 0) and rec["mad_scale"] > 0)
+    assert zero >= 1  # a non-zero mean absolute deviation is among the cases
+
+
 def test_boxcar_snr_loc_scale_options(orc):
     """The S/N oracle's two z-scores: mean/std and median/IQR."""
     rng = np.random.default_rng(3)
