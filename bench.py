@@ -391,6 +391,8 @@ def run_gpu(args, rank, world, local):
             "metric": c3["metric"], "value": c3["value"], "unit": UNIT,
             "plain_per_call": c3["plain_per_call"]["value"],
             "served_over_plain": c3["served_over_plain"], "beams": 64,
+            "batched_brute_force": c3["batched_brute_force"]["value"],
+            "batched_brute_force_over_plain": c3["batched_brute_force"]["over_plain"],
             "ms_per_step": c3["ms_per_step"], "steps": c3["steps"]}
         torch.cuda.empty_cache()
         c4 = workloads.measure_c4(args.chunks, args.budget_gb, local, 1)

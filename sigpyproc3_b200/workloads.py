@@ -287,6 +287,7 @@ def measure_c3(steps: int, warmup: int, beams: int, batch: int, rank: int, world
         torch.cuda.synchronize()
         t_plain += time.perf_counter() - t0
     plain = u_plain / t_plain
+    brute = _c3_batched_brute_force(plan, h, lens[:min(batch, nbeams)], factors, widths, g)
     return dict(metric="DM-trial x samples/s, config 3 (batched two-stage subband search + S/N)",
               value=value, unit=UNIT, n_gpus=world, steps=steps, warmup=warmup,
               ms_per_step=ms_max, higher_is_better=True, scaling="weak", vs_baseline=None,
@@ -299,7 +300,67 @@ def measure_c3(steps: int, warmup: int, beams: int, batch: int, rank: int, world
                               "per (beam, DM), brute force over 1024 channels",
                               "sample": f"{nsub_beams} beams x {nsub_dms} DMs"},
               served_over_plain=value / plain, max_snr=max(peaks) if peaks else None,
+              batched_brute_force={**brute, "over_plain": brute["value"] / plain},
               gpu_launches=None)
+
+
+def _c3_batched_brute_force(plan, h, lens, factors, widths, g) -> dict:
+    """The plain path's algorithm (every trial over every channel) with the
+    batching alone: all trials of a batch of beams in one persistent
+    work-list launch, then S/N per beam.  Isolates what batching adds over
+    per-call dedispersion; the two-stage subband search adds the rest."""
+    from .batch import WorkList, num_variants, variant_cfg
+    from .search import boxcar_snr
+
+    lib = _lib.load()
+    d_all = np.atleast_2d(h.get_dmdelays(plan.dms)).astype(np.int32)
+    maxd = int(d_all.max())
+    dd = torch.from_numpy(d_all).cuda()
+    wl = None
+    for v in range(num_variants(8)):  # the first kernel whose slot holds the spread
+        cand = WorkList(8, v)
+        slot = cand.slot_words(cand.span_of(d_all))
+        if slot > 0 and lib.spp_wl_smem_bytes(8, _lib.ACC_KAHAN32, v, slot) <= 227 * 1024:
+            wl = cand
+            break
+    span = wl.span_of(d_all)
+    slot = wl.slot_words(span)
+    beams = []
+    for i, n in enumerate(lens):
+        n = int(n)
+        nv = n - maxd
+        raw = synth.gauss_u8_device(n * g.nchans, 3000 + i, 96.0, 12.0)
+        halo, pitch, rpc = wl.layout(nv, 0, maxd, slot)
+        planar = torch.empty(g.nchans * rpc * pitch, dtype=torch.int32, device="cuda")
+        out = torch.empty((d_all.shape[0], nv), dtype=torch.int32, device="cuda")
+        wl.add_job(planar_ptr=planar.data_ptr(), pitch_w=pitch, halo=halo, nchans=g.nchans,
+                   delays_dev=dd, delays_host=d_all, out_ptr=out.data_ptr(),
+                   out_stride=out.stride(0), out_start=0, out_elem=4, nvalid=nv,
+                   out_kind=_lib.OUT_I32)
+        beams.append((raw, n, halo, planar, pitch, out))
+    wl.finalize(span)
+
+    def run():
+        for raw, n, halo, planar, pitch, _ in beams:
+            wl.corner_turn(raw, _lib.BITORDER_BIG, g.nchans, n, halo, planar, pitch)
+        wl.launch()
+        for *_, out in beams:
+            boxcar_snr(out, widths=widths, factors=factors)
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = _events()
+    e0.record()
+    run()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    assert int(wl.status[0].item()) == 0
+    units = sum(d_all.shape[0] * out.shape[1] for *_, out in beams)
+    return {"value": units / (ms / 1e3), "unit": UNIT, "ms": ms, "beams": len(beams),
+            "kernel": variant_cfg(8, _lib.ACC_KAHAN32, wl.variant),
+            "path": "corner turns + one persistent work-list launch over every beam's 512 trials "
+                    "x 1024 channels + S/N per beam"}
 
 
 def run_c4(args, rank, world, local, emit) -> None:
