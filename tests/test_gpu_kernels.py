@@ -156,6 +156,60 @@ def test_dmt_plan_all_variants(torch_cuda, orc, nbits, wide):
     np.testing.assert_array_equal(out.cpu().numpy(), expect.astype(np.float32))
 
 
+@pytest.mark.parametrize("nbits", [1, 2, 4, 8])
+def test_dmt_plan_negative_delays_all_variants(torch_cuda, orc, nbits):
+    """Delays referenced to the band centre (negative in its upper half, so
+    samples before the block wrap as numba's negative indices) through every
+    kernel variant, bit-sliced and SIMD, against the oracle; 72 channels (a
+    partial last slab of 16 or 32)."""
+    torch = torch_cuda
+    from sigpyproc3_b200.dedisp import DMTPlan
+
+    nchans, nsamps, ndm = 72, 3000, 21
+    rng = np.random.default_rng(40 + nbits)
+    vals = rng.integers(0, 1 << nbits, size=nsamps * nchans, dtype=np.uint8)
+    raw = vals if nbits == 8 else _pack(vals, nbits, "big")
+    d = np.atleast_2d(_geom_delays(nchans, np.linspace(0, 80, ndm), ref="fcenter"))
+    assert d.min() < 0 < d.max()
+    nvalid = nsamps - int(np.abs(d).max())
+    expect = orc.dmt(vals, d, nchans, nsamps, nvalid)
+    plan = DMTPlan(d, nchans, nsamps, nbits=nbits, out_dtype=torch.int32)
+    rawd = torch.from_numpy(raw).cuda()
+    sliced = 0
+    for v in range(plan.num_variants):
+        plan.set_variant(v)
+        out = plan.execute(rawd, nsamps, check=True)
+        np.testing.assert_array_equal(out.cpu().numpy(), expect, err_msg=str(plan.describe()))
+        sliced += plan.describe()["bit_sliced"]
+    plan.close()
+    assert sliced >= 1
+
+
+@pytest.mark.parametrize("nbits", [2, 4, 8])
+def test_dmt_plan_roll_mode_integer(torch_cuda, orc, nbits):
+    """Roll mode (kernels.dmt_block: circular shifts by +delay) on packed
+    integer samples through every variant, against the oracle's float32 roll
+    of the same integer values (exact)."""
+    torch = torch_cuda
+    from sigpyproc3_b200.dedisp import DMTPlan
+
+    nchans, nsamps, ndm = 64, 2048, 12
+    rng = np.random.default_rng(60 + nbits)
+    vals = rng.integers(0, 1 << nbits, size=nsamps * nchans, dtype=np.uint8)
+    raw = vals if nbits == 8 else _pack(vals, nbits, "big")
+    d = np.atleast_2d(_geom_delays(nchans, np.linspace(0, 40, ndm)))
+    assert int(d.max()) < nsamps
+    expect = orc.dmt_roll(vals.astype(np.float32), d, nchans, nsamps)
+    plan = DMTPlan(d, nchans, nsamps, nbits=nbits, mode="roll", out_dtype=torch.int32)
+    rawd = torch.from_numpy(raw).cuda()
+    for v in range(plan.num_variants):
+        plan.set_variant(v)
+        out = plan.execute(rawd, nsamps, check=True)
+        np.testing.assert_array_equal(out.cpu().numpy().astype(np.float32), expect,
+                                      err_msg=str(plan.describe()))
+    plan.close()
+
+
 def test_dmt_plan_out_stride_and_offset(torch_cuda, orc):
     torch = torch_cuda
     from sigpyproc3_b200.dedisp import DMTPlan
