@@ -245,7 +245,7 @@ int spp_wl_corner_turn(int nbits, int acc, int variant, const void* in, int bito
   if (!in || !planar || nchans <= 0 || nsamps <= 0 || (pitch_w & 3) || halo < 0 || (nchans * nbits) % 8)
     return fail(SPP_ERR_ARG, "bad corner-turn arguments");
   dim3 grid((unsigned)ceil_div(nchans, planes_ct_chans(nbits)),
-            (unsigned)std::min<int64_t>(ceil_div(pitch_w, kCtWords), 65535));
+            (unsigned)std::min<int64_t>(ceil_div(pitch_w, kPlaneWords), 65535));
   const uint8_t* raw = static_cast<const uint8_t*>(in);
   uint32_t* pl = static_cast<uint32_t*>(planar);
   cudaStream_t st = stq(stream);

@@ -220,7 +220,7 @@ static int launch_corner_turn(int nb, const void* in, int bitorder, int64_t ncha
                               const float* bpass = nullptr, uint32_t* special = nullptr) {
   if (g.planes) {
     dim3 grid((unsigned)ceil_div(nchans, planes_ct_chans(nb)),
-              (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, kCtWords), 65535));
+              (unsigned)std::min<int64_t>(ceil_div(g.pitch_w, kPlaneWords), 65535));
     const uint8_t* raw = static_cast<const uint8_t*>(in);
     uint32_t* pl = static_cast<uint32_t*>(planar);
     if (nb == 1)

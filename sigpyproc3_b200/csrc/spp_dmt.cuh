@@ -67,9 +67,11 @@ __device__ __forceinline__ int64_t wrap_row(int64_t s, int64_t nsamps) {
 // ----------------------------------------------------------------------------
 constexpr int kCtChans = 64;
 constexpr int kCtWords = 16;
-// Channels per tile of the bit-plane corner turn: 8-bit data takes 32, so
-// the tile's raw bytes and its 8 plane rows per channel fit static shared memory.
-__host__ __device__ constexpr int planes_ct_chans(int nb) { return nb == 8 ? 32 : kCtChans; }
+// Tile of the bit-plane corner turn: 256 / nb channels (32 bytes of each raw
+// row: whole 32-byte sectors in) by kPlaneWords words of each plane row
+// (8 words = 32 bytes: whole sectors out), i.e. 256 raw rows.
+__host__ __device__ constexpr int planes_ct_chans(int nb) { return 256 / nb; }
+constexpr int kPlaneWords = 8;
 
 template <int NB>
 __global__ void __launch_bounds__(256)
@@ -1307,19 +1309,37 @@ k_dmt_bits_minb(const DmtArgs a) {
   dmt_bits_body<NB, P, DW, TW, STAGES, L, SLAB, SLOT>(a);
 }
 
+// 32 x 32 bit transpose across a warp: lane j holds row j (bit i = column
+// i); afterwards lane i holds column i (bit j = row j).  Five rounds, each
+// swapping the off-diagonal s x s blocks with the lane s apart.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const uint32_t m = s == 16 ? 0x0000FFFFu : s == 8 ? 0x00FF00FFu : s == 4 ? 0x0F0F0F0Fu
+                     : s == 2 ? 0x33333333u : 0x55555555u;  // bits whose index has bit s clear
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, s);
+    const bool up = (lane & s) != 0;
+    const uint32_t t = up ? (y >> s) : (y << s);
+    const uint32_t keep = up ? ~m : m;
+    x = (x & keep) | (t & ~keep);
+  }
+  return x;
+}
+
 // Corner turn into bit-plane rows (row c*NB + b: bit b of channel c, 32
-// samples per word).  CTA = 64 channels x 16 words (512 raw rows).
+// samples per word).  CTA = planes_ct_chans(NB) channels x kPlaneWords words
+// (256 raw rows).
 template <int NB>
 __global__ void __launch_bounds__(256)
 k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t nsamps,
                      int bitorder, int64_t halo, uint32_t* __restrict__ planar,
                      int64_t pitch_w) {
   constexpr int CC = planes_ct_chans(NB);
-  constexpr int RT = kCtWords * 32;
+  constexpr int RT = kPlaneWords * 32;
   constexpr int SB = CC * NB / 8;
   constexpr int SBP = SB + 4;
   __shared__ __align__(16) uint8_t s_raw[RT * SBP];
-  __shared__ uint32_t s_out[CC * NB][kCtWords + 1];
+  __shared__ uint32_t s_out[CC * NB][kPlaneWords + 1];
   const int64_t c0 = (int64_t)blockIdx.x * CC;
   const int nc = (int)((nchans - c0) < CC ? (nchans - c0) : CC);
   const int seg = (nc * NB + 7) / 8;
@@ -1327,10 +1347,28 @@ k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t ns
   const int64_t segstart = c0 * NB / 8;
   const bool vec = ((rowbytes & 3) == 0) && ((segstart & 3) == 0) && ((seg & 3) == 0) &&
                    ((reinterpret_cast<uintptr_t>(raw) & 3) == 0);
-  const int64_t ntw = (pitch_w + kCtWords - 1) / kCtWords;
+  const bool vec16 = ((rowbytes & 15) == 0) && ((segstart & 15) == 0) && ((seg & 15) == 0) &&
+                     ((reinterpret_cast<uintptr_t>(raw) & 15) == 0);
+  // plane words leave in 16-byte stores (pitches are multiples of 4 words and
+  // tiles start at multiples of 8)
+  const bool st16 = ((pitch_w & 3) == 0) && ((reinterpret_cast<uintptr_t>(planar) & 15) == 0);
+  const int64_t ntw = (pitch_w + kPlaneWords - 1) / kPlaneWords;
   for (int64_t by = blockIdx.y; by < ntw; by += gridDim.y) {
-    const int64_t w0 = by * kCtWords;
-    if (vec) {
+    const int64_t w0 = by * kPlaneWords;
+    if (vec16) {
+      const int nq = seg >> 4;
+      for (int idx = threadIdx.x; idx < RT * nq; idx += blockDim.x) {
+        const int r = idx / nq, k = idx - r * nq;
+        const int64_t row = wrap_row(w0 * 32 + r - halo, nsamps);
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (row >= 0) v = __ldg(reinterpret_cast<const uint4*>(raw + row * rowbytes + segstart) + k);
+        uint32_t* d = reinterpret_cast<uint32_t*>(s_raw + r * SBP + 16 * k);
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
+      }
+    } else if (vec) {
       const int nw = seg >> 2;
       for (int idx = threadIdx.x; idx < RT * nw; idx += blockDim.x) {
         const int r = idx / nw, k = idx - r * nw;
@@ -1347,27 +1385,36 @@ k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t ns
       }
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < CC * kCtWords; idx += blockDim.x) {
-      const int c = idx % CC, w = idx / CC;
-      uint32_t v[NB];
-#pragma unroll
-      for (int b = 0; b < NB; ++b) v[b] = 0;
-      if (c < nc) {
-        const int byte = (c * NB) / 8;
-#pragma unroll 8
-        for (int j = 0; j < 32; ++j) {
-          const uint32_t f = field_of<NB>(s_raw[(w * 32 + j) * SBP + byte], c, bitorder);
-#pragma unroll
-          for (int b = 0; b < NB; ++b) v[b] |= ((f >> b) & 1u) << j;
-        }
+    // one warp per (word w, 4-byte column group g): lane j loads the group's
+    // 32 bits of row 32w + j, a 32 x 32 bit transpose leaves in lane i bit i
+    // of all 32 rows -- the plane word (32 samples, LSB first) of the
+    // (channel, plane) that bit i of the packed bytes holds
+    {
+      constexpr int NG = SB / 4;  // column groups per row segment
+      const int lane = threadIdx.x & 31;
+      const int bi = lane >> 3, bb = lane & 7;
+      const int q = (bitorder == SPP_BITORDER_BIG) ? (7 - bb) / NB : bb / NB;
+      for (int task = threadIdx.x >> 5; task < kPlaneWords * NG; task += blockDim.x >> 5) {
+        const int w = task / NG, g = task - w * NG;
+        uint32_t x = *reinterpret_cast<const uint32_t*>(s_raw + (w * 32 + lane) * SBP + 4 * g);
+        x = warp_transpose32(x, lane);
+        const int c = (4 * g + bi) * (8 / NB) + q;
+        s_out[c * NB + bb % NB][w] = x;
       }
-#pragma unroll
-      for (int b = 0; b < NB; ++b) s_out[c * NB + b][w] = v[b];
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < CC * NB * kCtWords; idx += blockDim.x) {
-      const int w = idx % kCtWords, rr = idx / kCtWords;
-      if (rr < nc * NB && w0 + w < pitch_w) planar[(c0 * NB + rr) * pitch_w + w0 + w] = s_out[rr][w];
+    if (st16) {
+      for (int idx = threadIdx.x; idx < CC * NB * (kPlaneWords / 4); idx += blockDim.x) {
+        const int w = 4 * (idx % (kPlaneWords / 4)), rr = idx / (kPlaneWords / 4);
+        if (rr < nc * NB && w0 + w < pitch_w)
+          *reinterpret_cast<uint4*>(planar + (c0 * NB + rr) * pitch_w + w0 + w) =
+              make_uint4(s_out[rr][w], s_out[rr][w + 1], s_out[rr][w + 2], s_out[rr][w + 3]);
+      }
+    } else {
+      for (int idx = threadIdx.x; idx < CC * NB * kPlaneWords; idx += blockDim.x) {
+        const int w = idx % kPlaneWords, rr = idx / kPlaneWords;
+        if (rr < nc * NB && w0 + w < pitch_w) planar[(c0 * NB + rr) * pitch_w + w0 + w] = s_out[rr][w];
+      }
     }
     __syncthreads();
   }
