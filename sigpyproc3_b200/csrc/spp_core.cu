@@ -84,6 +84,7 @@ struct Variant {
   int single;  // 1: meant for one DM (time-split warps)
   int planes;  // 1: bit-sliced kernel over bit-plane rows (R = words per thread)
   int slot;    // > 0: kernel compiled for exactly this slot width (words)
+  int pairs = 0;  // 1: 2-bit channel-pair kernel over pair-sum rows (three planes)
 };
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES, int ACC>
@@ -105,6 +106,18 @@ static Variant mkb() {
   return Variant{NB, 0, P, DW, TW, SLAB, STAGES, fn, 0, 1, SLOT};
 }
 
+// Channel-pair kernels (2-bit data): SLAB pairs per slab, two staged rows
+// per pair.
+template <int P, int DW, int TW, int STAGES, int SLAB, int SLOT = 0, int MINB = 0>
+static Variant mkp() {
+  constexpr int L = BitsLevels<3>::kLevels;
+  void (*fn)(const DmtArgs) = &k_dmt_pairs<P, DW, TW, STAGES, L, SLAB, SLOT>;
+  if constexpr (MINB > 0) fn = &k_dmt_pairs_minb<P, DW, TW, STAGES, L, SLAB, SLOT, MINB>;
+  Variant v{2, 0, P, DW, TW, SLAB, STAGES, fn, 0, 1, SLOT};
+  v.pairs = 1;
+  return v;
+}
+
 #define SPP_INT_VARIANTS(NB)                    \
   mk<NB, 2, 8, 1, 64, 3, 0>(0), mk<NB, 1, 8, 1, 64, 3, 0>(0), mk<NB, 2, 4, 2, 64, 3, 0>(0), \
       mk<NB, 1, 16, 1, 64, 3, 0>(0), mk<NB, 2, 1, 4, 64, 3, 0>(1), mk<NB, 1, 1, 4, 64, 3, 0>(1)
@@ -119,6 +132,10 @@ static const std::vector<Variant>& variants() {
       mkb<2, 3, 8, 1, 2, 32, 112, 3>(), mkb<2, 3, 8, 1, 2, 32, 112, 2>(),
       mkb<2, 2, 8, 1, 2>(), mkb<2, 2, 8, 1, 3, 32>(), mkb<2, 2, 8, 1, 2, 32>(),
       mkb<2, 4, 8, 1, 2, 32>(), mkb<2, 2, 16, 1, 2, 32>(), mkb<2, 1, 8, 1, 3>(),
+      // channel pairs summed once per relative delay (2-bit DM grids whose
+      // adjacent channels differ by few distinct delays)
+      mkp<3, 8, 1, 2, 8, 112, 3>(), mkp<3, 8, 1, 3, 8, 112, 3>(), mkp<3, 8, 1, 2, 16, 112, 2>(),
+      mkp<2, 8, 1, 2, 16, 80, 3>(), mkp<3, 8, 1, 2, 16>(), mkp<2, 8, 1, 3, 8>(),
       mkb<1, 2, 8, 1, 2, 32, 80>(), mkb<1, 2, 8, 1, 2, 32, 128>(),
       mkb<1, 2, 8, 1, 2>(), mkb<1, 2, 8, 1, 3, 32>(), mkb<1, 4, 8, 1, 2, 32>(),
       SPP_INT_VARIANTS(1),
@@ -173,6 +190,7 @@ static int slot_words(const Variant& v, int32_t span) {
 }
 
 static int64_t smem_bytes(const Variant& v, int slot_w) {
+  if (v.pairs) return v.STAGES * pair_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
   if (v.planes) return v.STAGES * bits_stage_bytes(v.nb, v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
   return v.STAGES * dmt_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
 }
@@ -594,6 +612,13 @@ struct spp_dmt_plan {
   std::vector<int> cands;      // candidate variant indices
   std::vector<int32_t> spans;  // span per candidate
   int cur = 0;                 // index into cands
+  // channel pairs (2-bit): rows (pair k, relative offset r) and each DM's row
+  // per pair; empty when the table has too many distinct offsets
+  int64_t nprows = 0;
+  int2* d_pair_src = nullptr;      // device, nprows x (k, r)
+  std::vector<int32_t> pair_rows;  // host, ndm x nchans/2 (plan creation only)
+  // per candidate (nullptr unless a pair kernel): staging tables
+  std::vector<int2*> pair_off, pair_ent;
   // optional per-kernel timing: events (start, after corner turn, end) per execute
   bool timing = false;
   std::vector<cudaEvent_t> evpool;
@@ -613,6 +638,76 @@ static int plan_sign(const spp_dmt_plan* p) { return p->mode == SPP_MODE_ROLL ? 
 
 static int64_t plan_nvalid(const spp_dmt_plan* p, int64_t nsamps) {
   return p->mode == SPP_MODE_ROLL ? nsamps : nsamps - p->maxabs;
+}
+
+// Staging tables of a pair kernel with DW trials per tile, SLAB pairs per
+// slab and slot_w words per staged row.  Per (tile, slab): the DW x SLAB
+// decoded offsets (staged row x 3 x slot_w + word, bit shift) and the
+// 2 x SLAB staged rows (pair-sum row, window start word relative to the time
+// tile; -1: unused).  The window of pair k starts at the 4-word boundary at
+// or below the tile's smallest offset of channel 2k; tiles are multiples of
+// 128 samples, so the same tables serve every time tile.
+static int pair_tables(spp_dmt_plan* p, const int32_t* delays_host, int dw, int slab, int slot_w,
+                       int2** d_off, int2** d_ent) {
+  const int64_t np = p->nchans / 2, ndm = p->ndm;
+  const int64_t ntile = ceil_div(ndm, dw), nslab = ceil_div(np, slab);
+  const int sign = plan_sign(p);
+  const int64_t halo = round_up(std::max<int64_t>(0, -(int64_t)p->omin), 128);
+  std::vector<int2> off((size_t)(ntile * nslab * dw * slab), make_int2(0, 0));
+  std::vector<int2> ent((size_t)(ntile * nslab * 2 * slab), make_int2(-1, 0));
+  for (int64_t t = 0; t < ntile; ++t) {
+    for (int64_t k = 0; k < nslab; ++k) {
+      const int64_t blk = t * nslab + k;
+      int e = 0;
+      for (int64_t j = 0; j < slab && k * slab + j < np; ++j) {
+        const int64_t pr = k * slab + j;
+        int32_t dv[64], rv[64], u[3];
+        int nu = 0;
+        int32_t mn = INT32_MAX;
+        for (int i = 0; i < dw; ++i) {
+          const int64_t dm = std::min<int64_t>(t * dw + i, ndm - 1);
+          dv[i] = sign * delays_host[dm * p->nchans + 2 * pr];
+          rv[i] = p->pair_rows[dm * np + pr];
+          mn = std::min(mn, dv[i]);
+          bool seen = false;
+          for (int m = 0; m < nu; ++m) seen = seen || u[m] == rv[i];
+          if (!seen) {
+            if (nu == 3) return fail(SPP_ERR_UNSUPPORTED, "pair %lld: more than 3 rows in a tile", (long long)pr);
+            u[nu++] = rv[i];
+          }
+        }
+        if (e + nu > 2 * slab) return fail(SPP_ERR_UNSUPPORTED, "pair slab needs more than %d rows", 2 * slab);
+        std::sort(u, u + nu);
+        const int64_t wsrel = ((mn + halo) / 32) & ~int64_t(3);  // mn + halo >= 0
+        const int64_t base = wsrel * 32 - halo;
+        for (int m = 0; m < nu; ++m) ent[blk * 2 * slab + e + m] = make_int2(u[m], (int)wsrel);
+        for (int i = 0; i < dw; ++i) {
+          int m = 0;
+          while (u[m] != rv[i]) ++m;
+          const int64_t o = dv[i] - base;
+          off[(blk * dw + i) * slab + j] =
+              make_int2((int)((e + m) * 3 * slot_w + (o >> 5)), (int)(o & 31));
+        }
+        e += nu;
+      }
+    }
+  }
+  cudaError_t err = cudaMalloc(d_off, sizeof(int2) * off.size());
+  if (err == cudaSuccess) err = cudaMalloc(d_ent, sizeof(int2) * ent.size());
+  if (err == cudaSuccess)
+    err = cudaMemcpy(*d_off, off.data(), sizeof(int2) * off.size(), cudaMemcpyHostToDevice);
+  if (err == cudaSuccess)
+    err = cudaMemcpy(*d_ent, ent.data(), sizeof(int2) * ent.size(), cudaMemcpyHostToDevice);
+  return cuda_status(err, "pair staging tables");
+}
+
+static void free_pair_tables(spp_dmt_plan* p) {
+  for (int2* q : p->pair_off) if (q) cudaFree(q);
+  for (int2* q : p->pair_ent) if (q) cudaFree(q);
+  p->pair_off.clear();
+  p->pair_ent.clear();
+  if (p->d_pair_src) cudaFree(p->d_pair_src);
+  p->d_pair_src = nullptr;
 }
 
 extern "C" {
@@ -676,9 +771,82 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
     span_of_dw.emplace_back(dw, span);
     return span;
   };
+  // Channel pairs (2-bit data): pair k = channels (2k, 2k+1) summed at the
+  // relative offset r = o(2k+1) - o(2k), one row per (k, r) over all DMs
+  // (at most 12 rows per channel, else the pair kernels are not offered).
+  std::vector<int2> pair_src;
+  if (nbits == 2) {
+    const int64_t np = nchans / 2;
+    std::vector<int32_t> rlo(np, INT32_MAX), rhi(np, INT32_MIN);
+    for (int64_t d = 0; d < ndm; ++d) {
+      const int32_t* row = delays_host + d * nchans;
+      for (int64_t k = 0; k < np; ++k) {
+        const int32_t r = sign * (row[2 * k + 1] - row[2 * k]);
+        rlo[k] = std::min(rlo[k], r);
+        rhi[k] = std::max(rhi[k], r);
+      }
+    }
+    std::vector<int64_t> rbase(np);
+    int64_t nrows = 0;
+    for (int64_t k = 0; k < np; ++k) {
+      rbase[k] = nrows;
+      nrows += (int64_t)rhi[k] - rlo[k] + 1;
+    }
+    if (nrows <= 12 * nchans) {
+      pair_src.resize(nrows);
+      for (int64_t k = 0; k < np; ++k)
+        for (int32_t r = rlo[k]; r <= rhi[k]; ++r)
+          pair_src[rbase[k] + (r - rlo[k])] = make_int2((int)k, r);
+      p->pair_rows.resize(ndm * np);
+      for (int64_t d = 0; d < ndm; ++d) {
+        const int32_t* row = delays_host + d * nchans;
+        for (int64_t k = 0; k < np; ++k) {
+          const int32_t r = sign * (row[2 * k + 1] - row[2 * k]);
+          p->pair_rows[d * np + k] = (int32_t)(rbase[k] + (r - rlo[k]));
+        }
+      }
+      p->nprows = nrows;
+    }
+  }
+  // a pair kernel's stage holds 2 x slab rows: in every DM tile each pair
+  // may use up to three distinct rows, and each slab's pairs together at
+  // most 2 x slab
+  std::vector<std::pair<int64_t, bool>> pairs_of_shape;
+  auto pairs_fit = [&](int dw, int slab) -> bool {
+    if (p->nprows == 0) return false;
+    const int64_t key = (int64_t)dw << 16 | slab;
+    for (auto& e : pairs_of_shape)
+      if (e.first == key) return e.second;
+    const int64_t np = nchans / 2;
+    bool fit = true;
+    for (int64_t d0 = 0; d0 < ndm && fit; d0 += dw) {
+      const int64_t d1 = std::min<int64_t>(ndm, d0 + dw);
+      int64_t used = 0;
+      for (int64_t k = 0; k < np && fit; ++k) {
+        int32_t u[3];
+        int n = 0;
+        for (int64_t d = d0; d < d1 && fit; ++d) {
+          const int32_t r = p->pair_rows[d * np + k];
+          bool seen = false;
+          for (int i = 0; i < n; ++i) seen = seen || u[i] == r;
+          if (seen) continue;
+          if (n == 3) fit = false;
+          else u[n++] = r;
+        }
+        used += n;
+        if ((k + 1) % slab == 0 || k + 1 == np) {
+          if (used > 2 * slab) fit = false;
+          used = 0;
+        }
+      }
+    }
+    pairs_of_shape.emplace_back(key, fit);
+    return fit;
+  };
   for (int i = 0; i < (int)vs.size(); ++i) {
     const Variant& v = vs[i];
     if (v.nb != nbits || (nbits == 32 && v.acc != acc)) continue;
+    if (v.pairs && !pairs_fit(v.DW, v.SLAB)) continue;
     if (ndm == 1 ? !v.single : v.single) continue;
     if (v.planes && nchans * ((1 << nbits) - 1) >= (1 << bit_levels(nbits))) continue;
     const int32_t span = tile_span(v.DW);
@@ -696,6 +864,31 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
   if (e != cudaSuccess) { delete p; return cuda_status(e, "plan cudaMalloc"); }
   e = cudaMemcpy(p->d_delays, delays_host, sizeof(int32_t) * ndm * nchans, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) { cudaFree(p->d_delays); delete p; return cuda_status(e, "plan upload"); }
+  bool use_pairs = false;
+  for (int c : p->cands) use_pairs = use_pairs || vs[c].pairs;
+  p->pair_off.assign(p->cands.size(), nullptr);
+  p->pair_ent.assign(p->cands.size(), nullptr);
+  if (use_pairs) {
+    e = cudaMalloc(&p->d_pair_src, sizeof(int2) * pair_src.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(p->d_pair_src, pair_src.data(), sizeof(int2) * pair_src.size(),
+                     cudaMemcpyHostToDevice);
+    int rc = cuda_status(e, "plan pair rows");
+    for (size_t i = 0; i < p->cands.size() && rc == SPP_OK; ++i) {
+      const Variant& v = vs[p->cands[i]];
+      if (v.pairs)
+        rc = pair_tables(p, delays_host, v.DW, v.SLAB, slot_words(v, p->spans[i]), &p->pair_off[i],
+                         &p->pair_ent[i]);
+    }
+    if (rc != SPP_OK) {
+      free_pair_tables(p);
+      cudaFree(p->d_delays);
+      delete p;
+      return rc;
+    }
+  }
+  p->pair_rows.clear();
+  p->pair_rows.shrink_to_fit();
   *plan = p;
   return SPP_OK;
 }
@@ -705,6 +898,7 @@ int spp_dmt_plan_destroy(spp_dmt_plan* p) {
   int rc = SPP_OK;
   for (cudaEvent_t e : p->evpool) cudaEventDestroy(e);
   if (p->d_delays) rc = cuda_status(cudaFree(p->d_delays), "plan cudaFree");
+  free_pair_tables(p);
   delete p;
   return rc;
 }
@@ -727,7 +921,7 @@ int spp_dmt_plan_describe(const spp_dmt_plan* p, int32_t* cfg) {
   if (!p || !cfg) return fail(SPP_ERR_ARG, "null pointer");
   const Variant& v = variants()[p->cands[p->cur]];
   const int slot = slot_words(v, p->spans[p->cur]);
-  cfg[0] = v.nb | (v.planes << 8); cfg[1] = v.R; cfg[2] = v.DW; cfg[3] = v.TW; cfg[4] = v.SLAB;
+  cfg[0] = v.nb | (v.planes << 8) | (v.pairs << 9); cfg[1] = v.R; cfg[2] = v.DW; cfg[3] = v.TW; cfg[4] = v.SLAB;
   cfg[5] = v.STAGES;
   cfg[6] = (int32_t)tile_T(v);
   cfg[7] = (int32_t)smem_bytes(v, slot);
@@ -740,11 +934,16 @@ static Geometry plan_geometry(const spp_dmt_plan* p, int64_t nsamps, int* slot) 
   return geometry(v, p->nchans, nsamps, plan_nvalid(p, nsamps), p->omin, p->omax, *slot);
 }
 
+// pair-sum rows follow the channel rows in the workspace
+static int64_t pair_bytes(const spp_dmt_plan* p, const Geometry& g) {
+  return variants()[p->cands[p->cur]].pairs ? p->nprows * 3 * g.pitch_w * 4 : 0;
+}
+
 int64_t spp_dmt_plan_workspace_bytes(const spp_dmt_plan* p, int64_t nsamps) {
   if (!p) return -1;
   int slot;
   Geometry g = plan_geometry(p, nsamps, &slot);
-  return kStatusBytes + g.bytes;
+  return kStatusBytes + g.bytes + pair_bytes(p, g);
 }
 
 static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* out,
@@ -758,9 +957,10 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
     return fail(SPP_ERR_DELAY, "roll mode needs |delay| < nsamps");
   if (-(int64_t)p->omin > nsamps)
     return fail(SPP_ERR_DELAY, "negative offset %d reaches before the block", p->omin);
-  if (ws_bytes < kStatusBytes + g.bytes)
+  const int64_t pb = pair_bytes(p, g);
+  if (ws_bytes < kStatusBytes + g.bytes + pb)
     return fail(SPP_ERR_SIZE, "workspace %lld B < required %lld B", (long long)ws_bytes,
-                (long long)(kStatusBytes + g.bytes));
+                (long long)(kStatusBytes + g.bytes + pb));
   if (out_start < 0 || (p->ndm > 1 && out_stride < out_start + g.nvalid))
     return fail(SPP_ERR_SIZE, "out_stride %lld < out_start %lld + nvalid %lld",
                 (long long)out_stride, (long long)out_start, (long long)g.nvalid);
@@ -795,6 +995,19 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
   rc = launch_corner_turn(p->nbits, in, p->bitorder, p->nchans, nsamps, g, planar, st, zd_rows,
                           zd_chanwts, zd_bpass, special);
   if (rc) return rc;
+  if (v.pairs) {
+    // pair-sum rows from the channel planes: one row per (pair, offset)
+    uint32_t* pp = reinterpret_cast<uint32_t*>(ws + kStatusBytes + g.bytes);
+    const int64_t gy = ceil_div(g.pitch_w, 4 * 256);
+    if (gy > 65535 || p->nprows > INT32_MAX)
+      return fail(SPP_ERR_UNSUPPORTED, "pair rows: %lld words x %lld rows", (long long)g.pitch_w,
+                  (long long)p->nprows);
+    k_pair_sums2<<<dim3((unsigned)p->nprows, (unsigned)gy), 256, 0, st>>>(
+        static_cast<const uint32_t*>(planar), g.pitch_w, p->d_pair_src, pp);
+    rc = cuda_status(cudaGetLastError(), "pair sums launch");
+    if (rc) return rc;
+    planar = pp;
+  }
   if (p->timing) cudaEventRecord(ev[1], st);
   DmtArgs a{};
   a.planar = planar;
@@ -816,6 +1029,9 @@ static int dmt_run(const spp_dmt_plan* p, const void* in, int64_t nsamps, void* 
   a.nvalid = g.nvalid;
   a.status = reinterpret_cast<uint32_t*>(ws);
   a.special = special;
+  a.pair_off = p->pair_off[p->cur];
+  a.pair_ent = p->pair_ent[p->cur];
+  a.npairs = (int32_t)(p->nchans / 2);
   rc = launch_dmt(v, a, g.ntiles_t, p->ndm, st);
   if (rc) return rc;
   if (p->timing) cudaEventRecord(ev[2], st);

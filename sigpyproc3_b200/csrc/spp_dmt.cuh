@@ -316,6 +316,14 @@ struct DmtArgs {
   // of the block is a normal float32 (set by the corner turn); then part of
   // the conversions run on the integer pipe.  nullptr: conversion unit only.
   const uint32_t* special;
+  // channel-pair kernels (2-bit data): `planar` holds pair-sum rows of three
+  // bit planes; per (DM tile, slab of pairs) the plan precomputes each DM's
+  // decoded offsets (pair_off, DW x SLAB) and the rows to stage (pair_ent,
+  // 2 x SLAB entries of (row, window start word relative to the tile; row -1:
+  // unused))
+  const int2* pair_off;
+  const int2* pair_ent;
+  int32_t npairs;
 };
 
 template <int NB, int R, int DW, int TW, int SLAB, int STAGES>
@@ -976,11 +984,13 @@ struct BitsWords {
 // Levels of the carry-save network per sample width: a quad of four channels
 // leaves one carry word of weight 2^kQuad (4 x (2^NB - 1) < 2^kQuad); the
 // counter needs kLevels levels for sums of 4096 channels (4096 x (2^NB - 1)
-// < 2^kLevels for 1-, 2-, 4- and 8-bit samples).
+// < 2^kLevels for 1-, 2-, 4- and 8-bit samples).  NB = 3: sums of two 2-bit
+// channels (0..6, three planes); 2048 of them need the 2-bit data's 14 levels.
 template <int NB>
 struct BitsLevels {
-  static_assert(NB == 1 || NB == 2 || NB == 4 || NB == 8, "bit-sliced kernels take 1-8 bit samples");
-  static constexpr int kQuad = NB == 8 ? 10 : NB == 4 ? 6 : NB == 2 ? 4 : 2;
+  static_assert(NB == 1 || NB == 2 || NB == 3 || NB == 4 || NB == 8,
+                "bit-sliced kernels take 1-8 bit samples or 2-bit pair sums");
+  static constexpr int kQuad = NB == 8 ? 10 : NB == 4 ? 6 : NB == 3 ? 5 : NB == 2 ? 4 : 2;
   static constexpr int kLevels = NB == 8 ? 20 : NB == 4 ? 16 : 14;
 };
 
@@ -1142,6 +1152,10 @@ __device__ __forceinline__ void bits_slab(BitCounter<P, L>& cnt, const uint32_t*
   }
 }
 
+template <int P, int L>
+__device__ __forceinline__ void store_bits_counts(const BitCounter<P, L>& cnt, const DmtArgs& a,
+                                                  int dm, int64_t t0, int wbase);
+
 template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT>
 __device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
   using Sh = BitsShape<NB, P, DW, TW, SLAB>;
@@ -1261,7 +1275,13 @@ __device__ __forceinline__ void dmt_bits_body(const DmtArgs& a) {
     if (lane == 0) mbar_arrive(&empty[s]);
   }
   if (!ok || dm >= a.ndm) return;
-  // outputs: word p covers samples t0 + 32*(wbase + pos(p)) + i
+  store_bits_counts<P, L>(cnt, a, dm, t0, wbase);
+}
+
+// Counts of DM row dm: word p covers samples t0 + 32*(wbase + pos(p)) + i.
+template <int P, int L>
+__device__ __forceinline__ void store_bits_counts(const BitCounter<P, L>& cnt, const DmtArgs& a,
+                                                  int dm, int64_t t0, int wbase) {
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     const int64_t tb = t0 + 32LL * (wbase + BitsWords<P>::pos(p));
@@ -1421,7 +1441,246 @@ k_corner_turn_planes(const uint8_t* __restrict__ raw, int64_t nchans, int64_t ns
 }
 
 // ----------------------------------------------------------------------------
-// Persistent work-list version of the bit-sliced kernel (same items as
+// Channel-pair sums of 2-bit data.
+//
+// The transform's sum over channels is regrouped into pairs (2k, 2k+1):
+//   out[dm][t] = sum_k S_k,r[t + o(dm, 2k)],   S_k,r[t] = x[2k][t] + x[2k+1][t + r]
+// with r = o(dm, 2k+1) - o(dm, 2k).  Over a DM grid each pair sees few
+// distinct r (the delay difference of two adjacent channels), so every
+// (pair, r) row is summed once and shared by all DMs that use it: the DM
+// kernel then adds 3 bit planes per two channels instead of 4 -- the same
+// integers in another order, so the sums are exact.
+// ----------------------------------------------------------------------------
+
+// Pair-sum rows: row i = (pair k, offset r) = src[i]; its planes b = 0..2 are
+// rows 3i + b of `out` on the channel rows' grid (same halo and pitch).  Each
+// thread makes four consecutive words; partner words outside channel 2k+1's
+// row read as zero (such words feed no valid output).
+static __global__ void __launch_bounds__(256)
+k_pair_sums2(const uint32_t* __restrict__ planar, int64_t pitch_w, const int2* __restrict__ src,
+             uint32_t* __restrict__ out) {
+  const int64_t row = blockIdx.x;
+  const int2 kr = __ldg(src + row);
+  const int64_t w = ((int64_t)blockIdx.y * blockDim.x + threadIdx.x) * 4;
+  if (w >= pitch_w) return;
+  const uint32_t* a0 = planar + (int64_t)(2 * kr.x) * 2 * pitch_w;   // channel 2k, plane 0
+  const uint32_t* b0 = a0 + 2 * pitch_w;                              // channel 2k+1, plane 0
+  const int q = kr.y >> 5, s = kr.y & 31;                             // floor(r / 32), r mod 32
+  const uint4 al = *reinterpret_cast<const uint4*>(a0 + w);
+  const uint4 ah = *reinterpret_cast<const uint4*>(a0 + pitch_w + w);
+  uint32_t bl[5], bh[5];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const int64_t j = w + q + i;
+    const bool in = j >= 0 && j < pitch_w;
+    bl[i] = in ? __ldg(b0 + j) : 0u;
+    bh[i] = in ? __ldg(b0 + pitch_w + j) : 0u;
+  }
+  const uint32_t xl[4] = {al.x, al.y, al.z, al.w}, xh[4] = {ah.x, ah.y, ah.z, ah.w};
+  uint32_t s0[4], s1[4], s2[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t yl = __funnelshift_r(bl[i], bl[i + 1], s);
+    const uint32_t yh = __funnelshift_r(bh[i], bh[i + 1], s);
+    const uint32_t c0 = xl[i] & yl;  // x + y, two 2-bit numbers: ripple add
+    s0[i] = xl[i] ^ yl;
+    s1[i] = xh[i] ^ yh ^ c0;
+    s2[i] = (xh[i] & yh) | (xh[i] & c0) | (yh & c0);
+  }
+  uint32_t* o = out + row * 3 * pitch_w + w;
+  *reinterpret_cast<uint4*>(o) = make_uint4(s0[0], s0[1], s0[2], s0[3]);
+  *reinterpret_cast<uint4*>(o + pitch_w) = make_uint4(s1[0], s1[1], s1[2], s1[3]);
+  *reinterpret_cast<uint4*>(o + 2 * pitch_w) = make_uint4(s2[0], s2[1], s2[2], s2[3]);
+}
+
+// Shared memory per stage of the pair kernel: SLAB pairs x 2 staged rows x 3
+// planes x slot_w words, plus DW x SLAB decoded offsets.
+__host__ __device__ constexpr int64_t pair_stage_bytes(int slab, int slot_w, int dw) {
+  return (int64_t)slab * 2 * 3 * slot_w * 4 + (int64_t)dw * slab * 8;
+}
+
+// One slab of SLAB pairs (SLAB = 8, 16 or 32) through the counter: quads of
+// pairs through the three-plane network (carry of weight 32), their carries
+// folded pairwise, the slab's single carry rippled up.  off[j] holds the
+// staged row's start word (row included) and the bit shift.
+template <int P, int L, int SLAB, bool FULL>
+__device__ __forceinline__ void pairs_slab(BitCounter<P, L>& cnt, const uint32_t* __restrict__ sd,
+                                           const int2* __restrict__ off, int nc, int slot_w,
+                                           int wbase) {
+  static_assert(SLAB == 8 || SLAB == 16 || SLAB == 32, "slab of 8, 16 or 32 pairs");
+  constexpr int NQ = SLAB / 4;
+  constexpr int LQ = BitsLevels<3>::kQuad;
+  uint32_t pw[P], pa[P], cm[2][P];
+#pragma unroll
+  for (int i = 0; i < NQ; ++i) {
+    const uint32_t* base[4];
+    int sh[4];
+    bool live[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int j = 4 * i + q;
+      live[q] = FULL || j < nc;
+      const int2 ow = live[q] ? off[j] : make_int2(0, 0);
+      sh[q] = ow.y;
+      base[q] = sd + ow.x + wbase;
+    }
+    uint32_t carry[3][4];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      uint32_t x[3][4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          uint32_t lo = 0u, hi = 0u;
+          if (live[q]) {
+            if constexpr (BitsWords<P>::kContig) {
+              lo = p == 0 ? base[q][b * slot_w] : carry[b][q];
+              hi = base[q][b * slot_w + p + 1];
+              carry[b][q] = hi;
+            } else {
+              lo = base[q][b * slot_w + 32 * p];
+              hi = base[q][b * slot_w + 32 * p + 1];
+            }
+          }
+          x[b][q] = __funnelshift_r(lo, hi, sh[q]);
+        }
+      }
+      auto word = [&](int b, int q) -> uint32_t { return x[b][q]; };
+      uint32_t cq;
+      QuadLevel<P, L, 3, 0, 0>::run(cnt, p, word, nullptr, cq);  // weight 32
+      if constexpr (NQ == 2) {
+        if (i == 0) {
+          pw[p] = cq;
+        } else {
+          uint32_t c6;
+          csa(cnt.A[p][LQ], pw[p], cq, c6);
+          cnt.ripple(p, LQ + 1, c6);
+        }
+      } else {
+        const int m = i / 4;  // group of four quads (16 pairs)
+        if (i % 4 == 0 || i % 4 == 2) {
+          pw[p] = cq;
+        } else if (i % 4 == 1) {
+          csa(cnt.A[p][LQ], pw[p], cq, pa[p]);
+        } else {
+          uint32_t pb;
+          csa(cnt.A[p][LQ], pw[p], cq, pb);
+          csa(cnt.A[p][LQ + 1], pa[p], pb, cm[m][p]);  // weight 128
+        }
+      }
+    }
+  }
+  if constexpr (NQ == 4) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) cnt.ripple(p, LQ + 2, cm[0][p]);
+  } else if constexpr (NQ == 8) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      uint32_t top;
+      csa(cnt.A[p][LQ + 2], cm[0][p], cm[1][p], top);
+      cnt.ripple(p, LQ + 3, top);
+    }
+  }
+}
+
+// DM-time transform over pair-sum rows.  CTA = DW DMs x one time tile, as
+// the bit-sliced kernel; a slab is SLAB pairs.  The DW DMs read one to three
+// distinct rows of a pair, 2 x SLAB rows per slab at most (the plan admits
+// the kernel only for tables where that holds).  Time tiles are multiples of
+// 128 samples, so where each DM reads within the staged windows does not
+// depend on the tile: the plan precomputes it per (DM tile, slab), and the
+// producer only issues bulk copies -- the offsets block and up to 2 x SLAB
+// rows of three planes.
+template <int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT>
+__device__ __forceinline__ void dmt_pairs_body(const DmtArgs& a) {
+  using Sh = BitsShape<3, P, DW, TW, SLAB>;
+  constexpr int NWC = Sh::kNwc;
+  constexpr int T = Sh::kT;
+  static_assert(2 * SLAB <= 32, "one producer lane per staged row");
+  static_assert(T % 128 == 0, "tile-independent staging needs 128-sample tiles");
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint32_t* sdata = reinterpret_cast<uint32_t*>(smem);
+  int2* soff = reinterpret_cast<int2*>(sdata + (int64_t)STAGES * SLAB * 6 * a.slot_w);
+  uint64_t* full = reinterpret_cast<uint64_t*>(soff + STAGES * DW * SLAB);
+  uint64_t* empty = full + STAGES;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int dm0 = blockIdx.x * DW;
+  const int64_t t0 = (int64_t)blockIdx.y * T;
+  const int nslab = (a.npairs + SLAB - 1) / SLAB;
+
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NWC);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == NWC) {
+    // producer: lane e stages row entry e of the slab
+    const uint32_t* planar = static_cast<const uint32_t*>(a.planar);
+    const int2* toff = a.pair_off + (int64_t)blockIdx.x * nslab * DW * SLAB;
+    const int2* tent = a.pair_ent + (int64_t)blockIdx.x * nslab * 2 * SLAB;
+    const int64_t tw0 = t0 / 32;
+    for (int k = 0; k < nslab; ++k) {
+      const int s = k % STAGES;
+      const int2 en = lane < 2 * SLAB ? __ldg(tent + (int64_t)k * 2 * SLAB + lane) : make_int2(-1, 0);
+      if (k >= STAGES && !mbar_wait(&empty[s], ((k / STAGES) - 1) & 1, a.status)) break;
+      const uint32_t nrow = __popc(__ballot_sync(0xffffffffu, en.x >= 0));
+      if (lane == 0)
+        mbar_arrive_expect_tx(&full[s], (uint32_t)(DW * SLAB * 8) + nrow * 3u * (uint32_t)a.slot_w * 4u);
+      __syncwarp();
+      if (lane == 0)
+        bulk_g2s(soff + s * DW * SLAB, toff + (int64_t)k * DW * SLAB, DW * SLAB * 8, &full[s]);
+      if (en.x >= 0) {
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+          bulk_g2s(sdata + (((int64_t)s * 2 * SLAB + lane) * 3 + b) * a.slot_w,
+                   planar + ((int64_t)en.x * 3 + b) * a.pitch_w + tw0 + en.y, a.slot_w * 4u,
+                   &full[s]);
+      }
+    }
+    return;
+  }
+
+  // consumers: warp (dmw, tw); thread words w = wbase + BitsWords<P>::pos(p)
+  const int dmw = warp / TW, tw = warp % TW;
+  const int dm = dm0 + dmw;
+  const int wbase = BitsWords<P>::base(tw, lane);
+  BitCounter<P, L> cnt;
+  cnt.zero();
+  bool ok = true;
+  for (int k = 0; k < nslab; ++k) {
+    const int s = k % STAGES;
+    if (!mbar_wait(&full[s], (k / STAGES) & 1, a.status)) { ok = false; break; }
+    const int nc = min(SLAB, a.npairs - k * SLAB);
+    const uint32_t* sd = sdata + (int64_t)s * SLAB * 6 * a.slot_w;
+    const int2* off = soff + (s * DW + dmw) * SLAB;
+    const int slot_w = SLOT > 0 ? SLOT : a.slot_w;
+    if (nc == SLAB) pairs_slab<P, L, SLAB, true>(cnt, sd, off, nc, slot_w, wbase);
+    else pairs_slab<P, L, SLAB, false>(cnt, sd, off, nc, slot_w, wbase);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+  }
+  if (!ok || dm >= a.ndm) return;
+  store_bits_counts<P, L>(cnt, a, dm, t0, wbase);
+}
+
+template <int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT = 0>
+__global__ void __launch_bounds__(BitsShape<3, P, DW, TW, SLAB>::kThreads)
+k_dmt_pairs(const DmtArgs a) {
+  dmt_pairs_body<P, DW, TW, STAGES, L, SLAB, SLOT>(a);
+}
+template <int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT, int MINB>
+__global__ void __launch_bounds__(BitsShape<3, P, DW, TW, SLAB>::kThreads, MINB)
+k_dmt_pairs_minb(const DmtArgs a) {
+  dmt_pairs_body<P, DW, TW, STAGES, L, SLAB, SLOT>(a);
+}
 // k_dmt_wl; planar rows are bit-plane rows, NB per channel).
 // ----------------------------------------------------------------------------
 template <int NB, int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT>

@@ -183,7 +183,8 @@ class DMTPlan:
         _lib.check(_lib.load().spp_dmt_plan_describe(self._h, cfg))
         keys = ("nbits", "R", "DW", "TW", "SLAB", "STAGES", "T", "smem")
         d = dict(zip(keys, list(cfg)))
-        d["bit_sliced"] = d["nbits"] >> 8
+        d["bit_sliced"] = (d["nbits"] >> 8) & 1
+        d["paired"] = (d["nbits"] >> 9) & 1
         d["nbits"] &= 0xFF
         return d
 
