@@ -313,10 +313,15 @@ def run_gpu(args, rank, world, local):
         prof = json.loads(tp.read_text())
         traffic = prof.get("k_dmt_c2_bytes_per_launch")
     adds = delays.shape[0] * nvalid * g.nchans
+    shape = plan.describe()
+    kname = ("k_dmt_pairs (channel pairs, bit-sliced)" if shape["paired"] else
+             "k_dmt_bits (bit-sliced)" if shape["bit_sliced"] else "k_dmt")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                "peak_source": peaks["source"], "kernel": "k_dmt_bits (bit-sliced)" if g.nbits <= 2 else "k_dmt",
-                "kernel_ms": dmt_s * 1e3, "corner_turn_ms": tk["ms_corner_turn"] / max(tk["n"], 1),
+                "peak_source": peaks["source"], "kernel": kname,
+                "kernel_ms": dmt_s * 1e3,
+                # the unpack + corner turn and, for the pair kernels, the pair sums
+                "corner_turn_ms": tk["ms_corner_turn"] / max(tk["n"], 1),
                 "int_adds_per_s": adds / dmt_s,
                 # pipe utilisation of the same kernel from the committed ncu capture
                 "pipes": {"alu": prof.get("alu_pipe_frac"), "lsu": prof.get("lsu_pipe_frac"),
