@@ -229,7 +229,10 @@ class DMTPlan:
                 table = {}
         if key in table and 0 <= table[key]["variant"] < self.num_variants:
             self.set_variant(table[key]["variant"])
-            return table[key]
+            # an entry written by a build with another variant list names
+            # another kernel: re-tune unless the recorded shape still matches
+            if table[key].get("shape") == self.describe():
+                return table[key]
         if out is None:
             out = torch.empty((self.ndm, self.nvalid(nsamps)), dtype=self.out_dtype,
                               device=raw.device)

@@ -178,3 +178,30 @@ def test_pairs_host_blocks(torch_cuda, orc):
         plan.execute_host(raw, nsamps, out, block_nsamps=4096)
         np.testing.assert_array_equal(out, expect, err_msg=str(plan.describe()))
     plan.close()
+
+
+def test_autotune_cache_checks_shape(torch_cuda, tmp_path):
+    """A cached choice counts only while the variant it names still has the
+    recorded tile shape (variant lists change between builds)."""
+    import json
+
+    torch = torch_cuda
+    from sigpyproc3_b200.dedisp import DMTPlan
+
+    nchans, nsamps = 64, 4096
+    d = _delays(nchans, np.linspace(0.0, 20.0, 16), 1500.0, -4.0, 64e-6)
+    rng = np.random.default_rng(3)
+    raw = torch.from_numpy(_pack2(rng.integers(0, 4, size=nsamps * nchans, dtype=np.uint8))).cuda()
+    cache = tmp_path / "tuned.json"
+    plan = DMTPlan(d, nchans, nsamps, nbits=2, out_dtype=torch.int32)
+    rec = plan.autotune(raw, nsamps, reps=1, cache=str(cache))
+    key = next(iter(json.loads(cache.read_text())))
+    assert plan.autotune(raw, nsamps, reps=1, cache=str(cache))["ms"] == rec["ms"]  # cache hit
+    table = json.loads(cache.read_text())
+    table[key]["shape"] = {"stale": 1}
+    table[key]["ms"] = -1.0
+    cache.write_text(json.dumps(table))
+    again = plan.autotune(raw, nsamps, reps=1, cache=str(cache))
+    assert again["ms"] >= 0.0 and again["shape"] == plan.describe()  # re-tuned
+    assert json.loads(cache.read_text())[key]["shape"] == plan.describe()
+    plan.close()
