@@ -197,9 +197,12 @@ int spp_dmt_plan_destroy(spp_dmt_plan* plan);
 /* valid output samples per row for an input of `nsamps` samples */
 int64_t spp_dmt_plan_nvalid(const spp_dmt_plan* plan, int64_t nsamps);
 int64_t spp_dmt_plan_workspace_bytes(const spp_dmt_plan* plan, int64_t nsamps);
-/* describe the chosen tiles: fills cfg[8] = {nbits | 256 * bit_sliced, R, DW,
- * TW, SLAB, STAGES, T (samples per tile), smem bytes}; bit_sliced = 1 when the
- * kernel counts over bit-plane rows (R = words per thread) */
+/* describe the chosen tiles: fills cfg[8] = {nbits | 256 * bit_sliced |
+ * 512 * paired, R, DW, TW, SLAB, STAGES, T (samples per tile), smem bytes};
+ * bit_sliced = 1 when the kernel counts over bit-plane rows (R = words per
+ * thread); paired = 1 for the 2-bit channel-pair kernels (SLAB counts pairs;
+ * the workspace then also holds one three-plane row per pair and relative
+ * delay, which spp_dmt_plan_workspace_bytes includes) */
 int spp_dmt_plan_describe(const spp_dmt_plan* plan, int32_t* cfg);
 /* override the tile shape (autotuner); variant index in [0, n) */
 int spp_dmt_plan_num_variants(const spp_dmt_plan* plan);

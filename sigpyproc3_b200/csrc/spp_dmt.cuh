@@ -1499,14 +1499,22 @@ __host__ __device__ constexpr int64_t pair_stage_bytes(int slab, int slot_w, int
   return (int64_t)slab * 2 * 3 * slot_w * 4 + (int64_t)dw * slab * 8;
 }
 
+// Level of the one carry word a slab of SLAB pairs leaves (quad carries of
+// weight 32 folded pairwise).
+template <int SLAB>
+__host__ __device__ constexpr int pairs_top_level() {
+  return BitsLevels<3>::kQuad + (SLAB == 8 ? 1 : SLAB == 16 ? 2 : 3);
+}
+
 // One slab of SLAB pairs (SLAB = 8, 16 or 32) through the counter: quads of
 // pairs through the three-plane network (carry of weight 32), their carries
-// folded pairwise, the slab's single carry rippled up.  off[j] holds the
-// staged row's start word (row included) and the bit shift.
+// folded pairwise; the slab's single carry (level pairs_top_level<SLAB>) is
+// returned in top[] for the caller to fold with the next slab's.  off[j]
+// holds the staged row's start word (row included) and the bit shift.
 template <int P, int L, int SLAB, bool FULL>
 __device__ __forceinline__ void pairs_slab(BitCounter<P, L>& cnt, const uint32_t* __restrict__ sd,
                                            const int2* __restrict__ off, int nc, int slot_w,
-                                           int wbase) {
+                                           int wbase, uint32_t (&top)[P]) {
   static_assert(SLAB == 8 || SLAB == 16 || SLAB == 32, "slab of 8, 16 or 32 pairs");
   constexpr int NQ = SLAB / 4;
   constexpr int LQ = BitsLevels<3>::kQuad;
@@ -1550,13 +1558,8 @@ __device__ __forceinline__ void pairs_slab(BitCounter<P, L>& cnt, const uint32_t
       uint32_t cq;
       QuadLevel<P, L, 3, 0, 0>::run(cnt, p, word, nullptr, cq);  // weight 32
       if constexpr (NQ == 2) {
-        if (i == 0) {
-          pw[p] = cq;
-        } else {
-          uint32_t c6;
-          csa(cnt.A[p][LQ], pw[p], cq, c6);
-          cnt.ripple(p, LQ + 1, c6);
-        }
+        if (i == 0) pw[p] = cq;
+        else csa(cnt.A[p][LQ], pw[p], cq, top[p]);  // weight 64
       } else {
         const int m = i / 4;  // group of four quads (16 pairs)
         if (i % 4 == 0 || i % 4 == 2) {
@@ -1573,14 +1576,10 @@ __device__ __forceinline__ void pairs_slab(BitCounter<P, L>& cnt, const uint32_t
   }
   if constexpr (NQ == 4) {
 #pragma unroll
-    for (int p = 0; p < P; ++p) cnt.ripple(p, LQ + 2, cm[0][p]);
+    for (int p = 0; p < P; ++p) top[p] = cm[0][p];
   } else if constexpr (NQ == 8) {
 #pragma unroll
-    for (int p = 0; p < P; ++p) {
-      uint32_t top;
-      csa(cnt.A[p][LQ + 2], cm[0][p], cm[1][p], top);
-      cnt.ripple(p, LQ + 3, top);
-    }
+    for (int p = 0; p < P; ++p) csa(cnt.A[p][LQ + 2], cm[0][p], cm[1][p], top[p]);
   }
 }
 
@@ -1654,6 +1653,10 @@ __device__ __forceinline__ void dmt_pairs_body(const DmtArgs& a) {
   const int wbase = BitsWords<P>::base(tw, lane);
   BitCounter<P, L> cnt;
   cnt.zero();
+  // slab carries are folded in pairs before they ripple up: one ripple per
+  // two slabs
+  constexpr int LT = pairs_top_level<SLAB>();
+  uint32_t hold[P];
   bool ok = true;
   for (int k = 0; k < nslab; ++k) {
     const int s = k % STAGES;
@@ -1662,12 +1665,28 @@ __device__ __forceinline__ void dmt_pairs_body(const DmtArgs& a) {
     const uint32_t* sd = sdata + (int64_t)s * SLAB * 6 * a.slot_w;
     const int2* off = soff + (s * DW + dmw) * SLAB;
     const int slot_w = SLOT > 0 ? SLOT : a.slot_w;
-    if (nc == SLAB) pairs_slab<P, L, SLAB, true>(cnt, sd, off, nc, slot_w, wbase);
-    else pairs_slab<P, L, SLAB, false>(cnt, sd, off, nc, slot_w, wbase);
+    uint32_t top[P];
+    if (nc == SLAB) pairs_slab<P, L, SLAB, true>(cnt, sd, off, nc, slot_w, wbase, top);
+    else pairs_slab<P, L, SLAB, false>(cnt, sd, off, nc, slot_w, wbase, top);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
+    if (k & 1) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        uint32_t c;
+        csa(cnt.A[p][LT], hold[p], top[p], c);
+        cnt.ripple(p, LT + 1, c);
+      }
+    } else {
+#pragma unroll
+      for (int p = 0; p < P; ++p) hold[p] = top[p];
+    }
   }
   if (!ok || dm >= a.ndm) return;
+  if (nslab & 1) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) cnt.ripple(p, LT, hold[p]);
+  }
   store_bits_counts<P, L>(cnt, a, dm, t0, wbase);
 }
 
