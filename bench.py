@@ -438,7 +438,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-block", type=int, default=65536,
+    ap.add_argument("--e2e-block", type=int, default=32768,
                     help="output samples per host-streaming block in the e2e leg")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true", help="skip the e2e row check")
