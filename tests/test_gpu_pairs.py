@@ -72,6 +72,8 @@ def test_pairs_c2_full_grid(torch_cuda, orc):
     rows = np.unique(np.r_[np.linspace(0, 1023, 60).astype(int), 1020, 1021, 1022, 1023])
     expect = orc.dmt(vals, d[rows], nchans, nsamps, nvalid)
     plan = DMTPlan(d, nchans, nsamps, nbits=2, bitorder="big", out_dtype=torch.int32)
+    # without autotuning the plan starts from a fixed-slot pair kernel here
+    assert plan.describe()["paired"] == 1, plan.describe()
     first = {}
 
     def check(got, desc):
