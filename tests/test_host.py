@@ -305,3 +305,39 @@ def test_counter_fits_bounds():
     assert counter_fits(sliced, 1, 16383) and not counter_fits(sliced, 1, 16384)
     assert counter_fits(sliced, 8, 4112) and not counter_fits(sliced, 8, 4113)
     assert counter_fits(simd, 4, 1 << 20)
+
+
+def test_channel_pair_regrouping_is_the_direct_sum(orc):
+    """The channel-pair kernels' identity, on the CPU: with pair rows
+    S_k,r[t] = x[2k][t] + x[2k+1][t + r] built once per (pair, relative
+    offset) and shared by every trial, sum_k S_k,r(dm)[t + o(dm, 2k)] equals
+    the oracle's direct sum over channels (kernels.dedisperse,
+    core/kernels.py:340-362) for every trial; the rows per pair and the
+    distinct rows per 8-trial tile are the quantities the plan checks."""
+    from sigpyproc3_b200.header import Header
+
+    nchans, nsamps = 64, 1500
+    h = Header(nchans=nchans, fch1=1500.0, foff=-2.0, tsamp=64e-6)
+    d = np.atleast_2d(h.get_dmdelays(np.linspace(0.0, 20.0, 24))).astype(np.int32)
+    nvalid = nsamps - int(d.max())
+    rng = np.random.default_rng(12)
+    x = rng.integers(0, 4, size=(nsamps, nchans), dtype=np.uint8)
+    expect = orc.dmt(x.ravel(), d, nchans, nsamps, nvalid)
+    r = d[:, 1::2] - d[:, 0::2]
+    rows = {}
+    for k in range(nchans // 2):
+        for rr in np.unique(r[:, k]):
+            s = x[:, 2 * k].astype(np.int32).copy()
+            part = np.zeros(nsamps, dtype=np.int32)
+            part[:nsamps - rr] = x[rr:, 2 * k + 1]
+            rows[(k, int(rr))] = s + part
+    got = np.zeros_like(expect)
+    for i in range(d.shape[0]):
+        for k in range(nchans // 2):
+            o = d[i, 2 * k]
+            got[i] += rows[(k, int(r[i, k]))][o:o + nvalid]
+    np.testing.assert_array_equal(got, expect)
+    assert len(rows) < 12 * nchans  # the plan's row budget
+    tiles = [max(len(np.unique(r[t:t + 8, k])) for k in range(nchans // 2))
+             for t in range(0, d.shape[0], 8)]
+    assert max(tiles) <= 3  # rows a tile of 8 trials reads per pair
