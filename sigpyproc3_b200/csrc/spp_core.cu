@@ -190,7 +190,9 @@ static int slot_words(const Variant& v, int32_t span) {
 }
 
 static int64_t smem_bytes(const Variant& v, int slot_w) {
-  if (v.pairs) return v.STAGES * pair_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
+  if (v.pairs)
+    return v.STAGES * pair_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8 +
+           pair_hi_bytes(v.R, v.DW * v.TW);
   if (v.planes) return v.STAGES * bits_stage_bytes(v.nb, v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
   return v.STAGES * dmt_stage_bytes(v.SLAB, slot_w, v.DW) + 8 + 2 * v.STAGES * 8;
 }

@@ -1499,6 +1499,14 @@ __host__ __device__ constexpr int64_t pair_stage_bytes(int slab, int slot_w, int
   return (int64_t)slab * 2 * 3 * slot_w * 4 + (int64_t)dw * slab * 8;
 }
 
+// The pair kernel keeps counter levels below kPairRegLevels in registers;
+// the upper levels, which change only when a carry ripples up (once per two
+// slabs), live in a per-thread slice of shared memory.
+constexpr int kPairRegLevels = 8;
+__host__ __device__ constexpr int64_t pair_hi_bytes(int p, int nwc) {
+  return (int64_t)(BitsLevels<3>::kLevels - kPairRegLevels) * p * nwc * 32 * 4;
+}
+
 // Level of the one carry word a slab of SLAB pairs leaves (quad carries of
 // weight 32 folded pairwise).
 template <int SLAB>
@@ -1651,8 +1659,37 @@ __device__ __forceinline__ void dmt_pairs_body(const DmtArgs& a) {
   const int dmw = warp / TW, tw = warp % TW;
   const int dm = dm0 + dmw;
   const int wbase = BitsWords<P>::base(tw, lane);
-  BitCounter<P, L> cnt;
+  // levels [0, LR) in registers, [LR, L) in this thread's shared slice
+  // (index ((l - LR) * P + p) * threads + thread: conflict-free)
+  constexpr int LR = kPairRegLevels;
+  static_assert(L > LR && pairs_top_level<SLAB>() < LR, "split counter levels");
+  uint32_t* shi = reinterpret_cast<uint32_t*>(empty + STAGES);
+  const int ct = threadIdx.x;
+  auto hi = [&](int l, int p) -> uint32_t& { return shi[((l - LR) * P + p) * (NWC * 32) + ct]; };
+#pragma unroll
+  for (int l = LR; l < L; ++l)
+#pragma unroll
+    for (int p = 0; p < P; ++p) hi(l, p) = 0u;
+  BitCounter<P, LR> cnt;
   cnt.zero();
+  // carry word c of weight 2^l0 up through the register and shared levels
+  auto ripple = [&](int p, int l0, uint32_t c) {
+#pragma unroll
+    for (int l = 0; l < LR; ++l) {
+      if (l < l0) continue;
+      uint32_t nc;
+      half(cnt.A[p][l], c, nc);
+      c = nc;
+    }
+#pragma unroll
+    for (int l = LR; l < L; ++l) {
+      if (c == 0u) break;
+      uint32_t& h = hi(l, p);
+      const uint32_t nc = h & c;
+      h ^= c;
+      c = nc;
+    }
+  };
   // slab carries are folded in pairs before they ripple up: one ripple per
   // two slabs
   constexpr int LT = pairs_top_level<SLAB>();
@@ -1666,8 +1703,8 @@ __device__ __forceinline__ void dmt_pairs_body(const DmtArgs& a) {
     const int2* off = soff + (s * DW + dmw) * SLAB;
     const int slot_w = SLOT > 0 ? SLOT : a.slot_w;
     uint32_t top[P];
-    if (nc == SLAB) pairs_slab<P, L, SLAB, true>(cnt, sd, off, nc, slot_w, wbase, top);
-    else pairs_slab<P, L, SLAB, false>(cnt, sd, off, nc, slot_w, wbase, top);
+    if (nc == SLAB) pairs_slab<P, LR, SLAB, true>(cnt, sd, off, nc, slot_w, wbase, top);
+    else pairs_slab<P, LR, SLAB, false>(cnt, sd, off, nc, slot_w, wbase, top);
     __syncwarp();
     if (lane == 0) mbar_arrive(&empty[s]);
     if (k & 1) {
@@ -1675,7 +1712,7 @@ __device__ __forceinline__ void dmt_pairs_body(const DmtArgs& a) {
       for (int p = 0; p < P; ++p) {
         uint32_t c;
         csa(cnt.A[p][LT], hold[p], top[p], c);
-        cnt.ripple(p, LT + 1, c);
+        ripple(p, LT + 1, c);
       }
     } else {
 #pragma unroll
@@ -1685,9 +1722,15 @@ __device__ __forceinline__ void dmt_pairs_body(const DmtArgs& a) {
   if (!ok || dm >= a.ndm) return;
   if (nslab & 1) {
 #pragma unroll
-    for (int p = 0; p < P; ++p) cnt.ripple(p, LT, hold[p]);
+    for (int p = 0; p < P; ++p) ripple(p, LT, hold[p]);
   }
-  store_bits_counts<P, L>(cnt, a, dm, t0, wbase);
+  BitCounter<P, L> all;
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+#pragma unroll
+    for (int l = 0; l < L; ++l) all.A[p][l] = l < LR ? cnt.A[p][l] : hi(l, p);
+  }
+  store_bits_counts<P, L>(all, a, dm, t0, wbase);
 }
 
 template <int P, int DW, int TW, int STAGES, int L, int SLAB, int SLOT = 0>
