@@ -892,13 +892,20 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
   p->pair_rows.clear();
   p->pair_rows.shrink_to_fit();
   // without autotuning, start from the first fixed-slot pair kernel when the
-  // table admits one (config 2: 17.5 ms against 22.1 ms for the first
-  // per-channel kernel at 2^18 outputs)
-  for (size_t i = 0; i < p->cands.size(); ++i)
-    if (vs[p->cands[i]].pairs && vs[p->cands[i]].slot > 0) {
-      p->cur = (int)i;
-      break;
-    }
+  // table admits one (config 2: 17.1 ms against 22.1 ms for the first
+  // per-channel kernel at 2^18 outputs) and its pair rows at nsamps_max stay
+  // within kPairDefaultBytes (longer blocks keep the pair kernels for explicit
+  // choice only: their rows grow with the block)
+  constexpr int64_t kPairDefaultBytes = 16ll << 30;
+  for (size_t i = 0; i < p->cands.size(); ++i) {
+    const Variant& v = vs[p->cands[i]];
+    if (!v.pairs || v.slot <= 0) continue;
+    const int slot = slot_words(v, p->spans[i]);
+    const Geometry g = geometry(v, nchans, nsamps_max, plan_nvalid(p, nsamps_max), p->omin,
+                                p->omax, slot);
+    if (p->nprows * 3 * g.pitch_w * 4 <= kPairDefaultBytes) p->cur = (int)i;
+    break;
+  }
   *plan = p;
   return SPP_OK;
 }
