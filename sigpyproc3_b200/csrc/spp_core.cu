@@ -618,8 +618,9 @@ struct spp_dmt_plan {
   // per pair; empty when the table has too many distinct offsets
   int64_t nprows = 0;
   int2* d_pair_src = nullptr;      // device, nprows x (k, r)
-  std::vector<int32_t> pair_rows;  // host, ndm x nchans/2 (plan creation only)
-  // per candidate (nullptr unless a pair kernel): staging tables
+  std::vector<int32_t> pair_rows;  // host, ndm x nchans/2
+  std::vector<int32_t> delays_h;   // host copy of the table while pair kernels are offered
+  // per candidate (nullptr until a pair kernel is first selected): staging tables
   std::vector<int2*> pair_off, pair_ent;
   // optional per-kernel timing: events (start, after corner turn, end) per execute
   bool timing = false;
@@ -700,7 +701,22 @@ static int pair_tables(spp_dmt_plan* p, const int32_t* delays_host, int dw, int 
     err = cudaMemcpy(*d_off, off.data(), sizeof(int2) * off.size(), cudaMemcpyHostToDevice);
   if (err == cudaSuccess)
     err = cudaMemcpy(*d_ent, ent.data(), sizeof(int2) * ent.size(), cudaMemcpyHostToDevice);
+  if (err != cudaSuccess) {  // leave both unset so a later selection retries
+    if (*d_off) cudaFree(*d_off);
+    if (*d_ent) cudaFree(*d_ent);
+    *d_off = nullptr;
+    *d_ent = nullptr;
+  }
   return cuda_status(err, "pair staging tables");
+}
+
+// Staging tables of candidate i, built the first time a pair kernel is
+// selected (plan creation for the initial choice, else set_variant).
+static int ensure_pair_tables(spp_dmt_plan* p, int i) {
+  const Variant& v = variants()[p->cands[i]];
+  if (!v.pairs || p->pair_off[i]) return SPP_OK;
+  return pair_tables(p, p->delays_h.data(), v.DW, v.SLAB, slot_words(v, p->spans[i]),
+                     &p->pair_off[i], &p->pair_ent[i]);
 }
 
 static void free_pair_tables(spp_dmt_plan* p) {
@@ -875,22 +891,18 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
     if (e == cudaSuccess)
       e = cudaMemcpy(p->d_pair_src, pair_src.data(), sizeof(int2) * pair_src.size(),
                      cudaMemcpyHostToDevice);
-    int rc = cuda_status(e, "plan pair rows");
-    for (size_t i = 0; i < p->cands.size() && rc == SPP_OK; ++i) {
-      const Variant& v = vs[p->cands[i]];
-      if (v.pairs)
-        rc = pair_tables(p, delays_host, v.DW, v.SLAB, slot_words(v, p->spans[i]), &p->pair_off[i],
-                         &p->pair_ent[i]);
-    }
+    const int rc = cuda_status(e, "plan pair rows");
     if (rc != SPP_OK) {
       free_pair_tables(p);
       cudaFree(p->d_delays);
       delete p;
       return rc;
     }
+    p->delays_h.assign(delays_host, delays_host + ndm * nchans);
+  } else {
+    p->pair_rows.clear();
+    p->pair_rows.shrink_to_fit();
   }
-  p->pair_rows.clear();
-  p->pair_rows.shrink_to_fit();
   // without autotuning, start from the first fixed-slot pair kernel when the
   // table admits one (config 2: 17.1 ms against 22.1 ms for the first
   // per-channel kernel at 2^18 outputs) and its pair rows at nsamps_max stay
@@ -905,6 +917,13 @@ int spp_dmt_plan_create(spp_dmt_plan** plan, int nbits, int bitorder, int64_t nc
                                 p->omax, slot);
     if (p->nprows * 3 * g.pitch_w * 4 <= kPairDefaultBytes) p->cur = (int)i;
     break;
+  }
+  const int trc = ensure_pair_tables(p, p->cur);
+  if (trc != SPP_OK) {
+    free_pair_tables(p);
+    cudaFree(p->d_delays);
+    delete p;
+    return trc;
   }
   *plan = p;
   return SPP_OK;
@@ -930,6 +949,8 @@ int spp_dmt_plan_num_variants(const spp_dmt_plan* p) { return p ? (int)p->cands.
 int spp_dmt_plan_set_variant(spp_dmt_plan* p, int variant) {
   if (!p) return fail(SPP_ERR_ARG, "null plan");
   if (variant < 0 || variant >= (int)p->cands.size()) return fail(SPP_ERR_ARG, "bad variant %d", variant);
+  const int rc = ensure_pair_tables(p, variant);
+  if (rc != SPP_OK) return rc;
   p->cur = variant;
   return SPP_OK;
 }
